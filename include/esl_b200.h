@@ -1,0 +1,141 @@
+/*
+ * esl_b200.h -- C ABI of the B200 (sm_100a) ExaStoLog stationary-distribution path.
+ *
+ * The reference (asmelko/paraExaStoLog) exposes this path as C++ classes; every
+ * entry point below names the reference interface it replaces.  Conventions:
+ *   - every function returns an int status (ESL_OK or a negative ESL_ERR_*) and
+ *     never exits the process; esl_last_error() gives the message (per thread);
+ *   - pointers named d_* are device pointers owned by the caller; everything
+ *     else is host memory;
+ *   - work is ordered on the stream given to esl_ctx_create; functions that
+ *     return host results synchronise that stream;
+ *   - state s is an n-bit integer, bit i is node i in bnet line order;
+ *     rates are [up_0, down_0, ..., up_{n-1}, down_{n-1}] (FP64).
+ */
+#ifndef ESL_B200_H
+#define ESL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESL_OK 0
+#define ESL_ERR_INVALID (-1)       /* bad argument or inconsistent sizes */
+#define ESL_ERR_PARSE (-2)         /* bnet / expression error */
+#define ESL_ERR_CUDA (-3)          /* CUDA runtime error */
+#define ESL_ERR_NOMEM (-4)         /* device or host allocation failed */
+#define ESL_ERR_TIMEOUT (-5)       /* a device fixpoint loop exceeded its budget */
+#define ESL_ERR_NOT_CONVERGED (-6) /* iterative solve missed its tolerance */
+#define ESL_ERR_TOO_LARGE (-7)     /* size beyond a documented limit */
+
+#define ESL_MAX_NODES 30
+
+typedef struct esl_ctx esl_ctx;     /* device + stream + scratch */
+typedef struct esl_model esl_model; /* parsed bnet: node names + DNF clauses */
+typedef struct esl_net esl_net;     /* device symbolic data for one (model, zero-rate pattern) */
+
+/* Solver method for the transient absorption and large terminal kernels. */
+#define ESL_METHOD_FP64 0    /* FP64 BiCGStab on the red-black reduced system */
+#define ESL_METHOD_MIXED 1   /* FP32 BiCGStab + FP64 iterative refinement */
+#define ESL_METHOD_DIRECT 2  /* FP64 block-triangular LU (dense per SCC block); small blocks only */
+
+typedef struct esl_solve_opts {
+    int method;            /* ESL_METHOD_* */
+    double tol;            /* relative residual target of the transient solve (default 1e-10) */
+    int max_iters;         /* iteration budget per Krylov solve (default 2000) */
+    int max_refine;        /* FP64 refinement steps for ESL_METHOD_MIXED (default 4) */
+    const double* d_warm;  /* optional warm start of the occupation vector, B x N (device), or NULL */
+} esl_solve_opts;
+
+typedef struct esl_report {
+    int iterations;        /* Krylov iterations (max over the batch) */
+    int refinements;       /* FP64 refinement steps taken */
+    double relres;         /* final relative residual (max over the batch) */
+    int converged;         /* 1 if every system met tol */
+} esl_report;
+
+const char* esl_last_error(void);
+int esl_version(void);
+
+/* ---- context -------------------------------------------------------- */
+int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out);
+int esl_ctx_destroy(esl_ctx* ctx);
+int esl_ctx_synchronize(esl_ctx* ctx);
+
+/* ---- model: replaces model_builder::construct_model (cuda/src/model.cpp:80-125)
+ *      and clause_t::get_positive_mask/get_negative_mask (cuda/src/model.cpp:8-21) */
+int esl_model_load(const char* path, esl_model** out);
+int esl_model_parse(const char* bnet_text, esl_model** out);
+int esl_model_free(esl_model* m);
+int esl_model_nodes(const esl_model* m, int* n);
+const char* esl_model_node_name(const esl_model* m, int i);
+int esl_model_node_index(const esl_model* m, const char* name, int* index);
+/* clause lists: off[n+1] prefixes into pos/neg; *total = clause count (arrays filled when cap >= total) */
+int esl_model_clauses(const esl_model* m, int32_t* off, uint32_t* pos, uint32_t* neg, int cap, int* total);
+
+/* ---- rates: replaces transition_rates::generate_uniform / generate_normal
+ *      (cuda/src/transition_rates.cpp:24-97); names not in the model -> ESL_ERR_INVALID,
+ *      negative rate -> ESL_ERR_INVALID.  rates_out has 2n entries. */
+int esl_rates_uniform(const esl_model* m, int n_up, const char* const* up_names, const double* up_vals,
+                      int n_down, const char* const* down_names, const double* down_vals, double* rates_out);
+int esl_rates_normal(const esl_model* m, double mean, double stddev, uint64_t seed, int n_up,
+                     const char* const* up_names, const double* up_vals, int n_down,
+                     const char* const* down_names, const double* down_vals, double* rates_out);
+
+/* ---- initial state: replaces initial_state::initial_state (cuda/src/initial_state.cu:7-60) */
+int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char* const* fixed_names,
+                      const int* fixed_values, double fixed_probability, double* d_x0);
+
+/* ---- transition table: replaces transition_table::construct_table
+ *      (cuda/src/transition_table.cu:121-174, sparse_utils.cu:14-32 coo2csc).
+ *      CSC by source: d_indptr[N+1], d_rows[nnz] = destinations (ascending within a
+ *      column), d_cols[nnz] = sources (may be NULL).  Call esl_table_nnz first. */
+int esl_table_nnz(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* nnz);
+int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32_t* d_indptr,
+                    int32_t* d_rows, int32_t* d_cols);
+/* per-state flip masks: bit i of d_out[s] = edge s -> s^(1<<i); of d_in[s] = edge s^(1<<i) -> s */
+int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in);
+
+/* ---- transition graph: replaces transition_graph::reorganize_vertices
+ *      (cuda/src/transition_graph.cu:39-202, kernels/transition_graph.cu:3-52).
+ *      Builds table masks, SCCs, terminal SCCs, levels and the reordering on the device. */
+int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net** out);
+/* same from a CSC table (any single-bit-flip graph, e.g. one produced by esl_table_build) */
+int esl_net_from_csc(esl_ctx* ctx, int n_nodes, const int32_t* d_indptr, const int32_t* d_rows,
+                     esl_net** out);
+int esl_net_free(esl_net* net);
+int esl_net_info(const esl_net* net, int* n_nodes, int* n_sccs, int* n_terminals, int* n_terminal_states);
+/* d_order[N] reordered vertices, d_offsets[n_sccs+1] SCC offsets (terminals first),
+ * d_levels[n_sccs] level of the SCC at each position (1 = terminal), d_labels[N] SCC label
+ * (min vertex of the SCC).  Any pointer may be NULL. */
+int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* d_offsets,
+                   int32_t* d_levels, int32_t* d_labels);
+/* 1 if the rate set has the zero pattern the net was built for */
+int esl_net_compatible(const esl_net* net, const double* rates, int* compatible);
+
+/* ---- solver: replaces solver::solve (cuda/src/solver.cu:311-334): terminal kernels
+ *      (solve_terminal_part :102-159), absorption (solve_nonterminal_part :205-300) and
+ *      x_inf = R (L x0) (compute_final_states :302-309), plus per-node marginals.
+ *      d_R[n_terminal_states] aligned with d_order; d_L[T x N] by original state (optional). */
+int esl_solve(esl_ctx* ctx, const esl_net* net, const double* d_rates, const double* d_x0,
+              double* d_x_inf, double* d_marginals, double* d_R, double* d_L,
+              const esl_solve_opts* opts, esl_report* report);
+
+/* Batched: B rate sets (d_rates B x 2n, same zero pattern) x R initial distributions
+ * (d_x0 R x N); outputs d_x_inf[B][R][N], d_marginals[B][R][n] (may be NULL). */
+int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R,
+                    const double* d_x0, double* d_x_inf, double* d_marginals,
+                    const esl_solve_opts* opts, esl_report* report);
+
+/* Host-memory end-to-end call: bnet text, rates (B x 2n) and x0 (R x N) on the host,
+ * results copied back to host buffers.  Builds and frees its own net. */
+int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,
+                   double* x_inf, double* marginals, const esl_solve_opts* opts, esl_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ESL_B200_H */

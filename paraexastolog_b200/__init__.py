@@ -1,0 +1,349 @@
+"""ExaStoLog stationary distributions on B200: Python host binding of libesl_b200.so.
+
+The library is the product: a C ABI (``include/esl_b200.h``) over hand-written
+sm_100a CUDA kernels.  This module binds it with ctypes; torch is used only for
+device memory and streams.  Importing it never falls back to another
+implementation: if the library is missing, ``lib()`` raises.
+
+Mirror of the reference's C++ API (``cuda/src/*.h``):
+    model_builder().construct_model(path)  -> Model.load(path)
+    transition_rates(model).generate_*      -> Model.rates_uniform / rates_normal
+    initial_state(nodes, fixed, values, p)  -> Model.initial_state
+    transition_table(...).construct_table   -> table()
+    transition_graph(...).reorganize_vertices -> Net.build / Net.export
+    solver(...).solve()                     -> solve(), solve_batch()
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from dataclasses import dataclass
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libesl_b200.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "esl_b200.h")
+
+ESL_OK = 0
+METHOD_FP64, METHOD_MIXED, METHOD_DIRECT = 0, 1, 2
+ERRORS = {-1: "INVALID", -2: "PARSE", -3: "CUDA", -4: "NOMEM", -5: "TIMEOUT", -6: "NOT_CONVERGED", -7: "TOO_LARGE"}
+
+_lib = None
+
+
+class EslError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("tol", C.c_double), ("max_iters", C.c_int), ("max_refine", C.c_int),
+                ("d_warm", C.c_void_p)]
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("relres", C.c_double), ("converged", C.c_int)]
+
+
+def header_functions() -> list:
+    """Names of the functions declared in include/esl_b200.h."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(esl_\w+)\s*\(", text, re.M)))
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m paraexastolog_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, cp, i32, u32, f64 = C.c_void_p, C.c_char_p, C.c_int32, C.c_uint32, C.c_double
+    P = C.POINTER
+    L.esl_last_error.restype = cp
+    L.esl_ctx_create.argtypes = [C.c_int, vp, P(vp)]
+    L.esl_ctx_destroy.argtypes = [vp]
+    L.esl_ctx_synchronize.argtypes = [vp]
+    L.esl_model_load.argtypes = [cp, P(vp)]
+    L.esl_model_parse.argtypes = [cp, P(vp)]
+    L.esl_model_free.argtypes = [vp]
+    L.esl_model_nodes.argtypes = [vp, P(C.c_int)]
+    L.esl_model_node_name.restype = cp
+    L.esl_model_node_name.argtypes = [vp, C.c_int]
+    L.esl_model_node_index.argtypes = [vp, cp, P(C.c_int)]
+    L.esl_model_clauses.argtypes = [vp, vp, vp, vp, C.c_int, P(C.c_int)]
+    L.esl_rates_uniform.argtypes = [vp, C.c_int, vp, vp, C.c_int, vp, vp, vp]
+    L.esl_rates_normal.argtypes = [vp, f64, f64, C.c_uint64, C.c_int, vp, vp, C.c_int, vp, vp, vp]
+    L.esl_initial_state.argtypes = [vp, vp, C.c_int, vp, vp, f64, vp]
+    L.esl_table_nnz.argtypes = [vp, vp, vp, P(C.c_int64)]
+    L.esl_table_build.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.esl_flip_masks.argtypes = [vp, vp, vp, vp, vp]
+    L.esl_net_build.argtypes = [vp, vp, vp, P(vp)]
+    L.esl_net_from_csc.argtypes = [vp, C.c_int, vp, vp, P(vp)]
+    L.esl_net_free.argtypes = [vp]
+    L.esl_net_info.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_int)]
+    L.esl_net_export.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.esl_net_compatible.argtypes = [vp, vp, P(C.c_int)]
+    L.esl_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, P(SolveOpts), P(Report)]
+    L.esl_solve_batch.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
+    L.esl_solve_host.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
+    _lib = L
+    return L
+
+
+def check(code: int):
+    if code != ESL_OK:
+        raise EslError(code, lib().esl_last_error().decode(errors="replace"))
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def _strs(names: Sequence[str]):
+    arr = (C.c_char_p * max(len(names), 1))(*[s.encode() for s in names])
+    return arr
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Context:
+    """Device, stream and scratch of the library (``cu_context`` in the reference)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        torch = _torch()
+        self.device = device
+        torch.cuda.set_device(device)
+        self.stream = stream if stream is not None else torch.cuda.current_stream(device)
+        h = C.c_void_p()
+        check(lib().esl_ctx_create(device, C.c_void_p(self.stream.cuda_stream), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().esl_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        check(lib().esl_ctx_synchronize(self._h))
+
+
+class Model:
+    """Parsed bnet model (``model_t``): node names and DNF clauses."""
+
+    def __init__(self, handle):
+        self._h = handle
+        n = C.c_int()
+        check(lib().esl_model_nodes(handle, C.byref(n)))
+        self.n = n.value
+        self.names = [lib().esl_model_node_name(handle, i).decode() for i in range(self.n)]
+
+    @classmethod
+    def parse(cls, text: str) -> "Model":
+        h = C.c_void_p()
+        check(lib().esl_model_parse(text.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path: str) -> "Model":
+        h = C.c_void_p()
+        check(lib().esl_model_load(path.encode(), C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.esl_model_free(self._h)
+            self._h = None
+
+    def clauses(self):
+        total = C.c_int()
+        check(lib().esl_model_clauses(self._h, None, None, None, 0, C.byref(total)))
+        off = np.zeros(self.n + 1, np.int32)
+        pos = np.zeros(max(total.value, 1), np.uint32)
+        neg = np.zeros(max(total.value, 1), np.uint32)
+        check(lib().esl_model_clauses(self._h, _ptr(off), _ptr(pos), _ptr(neg), total.value, C.byref(total)))
+        return off, pos[: total.value], neg[: total.value]
+
+    def rates_uniform(self, up: Optional[Dict[str, float]] = None, down: Optional[Dict[str, float]] = None) -> np.ndarray:
+        up, down = up or {}, down or {}
+        out = np.zeros(2 * self.n)
+        uv = np.array(list(up.values()), np.float64)
+        dv = np.array(list(down.values()), np.float64)
+        check(lib().esl_rates_uniform(self._h, len(up), _strs(list(up)), _ptr(uv), len(down), _strs(list(down)),
+                                      _ptr(dv), _ptr(out)))
+        return out
+
+    def rates_normal(self, mean: float, std: float, seed: int = 0, up=None, down=None) -> np.ndarray:
+        up, down = up or {}, down or {}
+        out = np.zeros(2 * self.n)
+        uv = np.array(list(up.values()), np.float64)
+        dv = np.array(list(down.values()), np.float64)
+        check(lib().esl_rates_normal(self._h, mean, std, seed, len(up), _strs(list(up)), _ptr(uv), len(down),
+                                     _strs(list(down)), _ptr(dv), _ptr(out)))
+        return out
+
+    def initial_state(self, ctx: Context, fixed: Sequence[str] = (), values: Sequence[int] = (), p: float = 1.0):
+        torch = _torch()
+        x0 = torch.empty(1 << self.n, dtype=torch.float64, device=f"cuda:{ctx.device}")
+        vals = np.array([int(bool(v)) for v in values], np.int32)
+        check(lib().esl_initial_state(ctx._h, self._h, len(fixed), _strs(list(fixed)), _ptr(vals), float(p), _ptr(x0)))
+        ctx.synchronize()
+        return x0
+
+
+def table(ctx: Context, model: Model, rates: np.ndarray, with_cols: bool = True):
+    """CSC transition table (indptr, rows, cols) as int32 device tensors."""
+    torch = _torch()
+    rates = np.ascontiguousarray(rates, np.float64)
+    nnz = C.c_int64()
+    check(lib().esl_table_nnz(ctx._h, model._h, _ptr(rates), C.byref(nnz)))
+    dev = f"cuda:{ctx.device}"
+    indptr = torch.empty((1 << model.n) + 1, dtype=torch.int32, device=dev)
+    rows = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+    cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev) if with_cols else None
+    check(lib().esl_table_build(ctx._h, model._h, _ptr(rates), _ptr(indptr), _ptr(rows), _ptr(cols)))
+    return indptr, rows[: nnz.value], (cols[: nnz.value] if with_cols else None)
+
+
+def flip_masks(ctx: Context, model: Model, rates: np.ndarray):
+    torch = _torch()
+    rates = np.ascontiguousarray(rates, np.float64)
+    dev = f"cuda:{ctx.device}"
+    F = torch.empty(1 << model.n, dtype=torch.int32, device=dev)
+    G = torch.empty(1 << model.n, dtype=torch.int32, device=dev)
+    check(lib().esl_flip_masks(ctx._h, model._h, _ptr(rates), _ptr(F), _ptr(G)))
+    return F, G
+
+
+class Net:
+    """Device symbolic data of one (model, zero-rate pattern): masks, SCCs, order."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self._h = handle
+        n, s, t, ts = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().esl_net_info(handle, C.byref(n), C.byref(s), C.byref(t), C.byref(ts)))
+        self.n, self.n_sccs, self.T, self.terminal_states = n.value, s.value, t.value, ts.value
+        self.N = 1 << self.n
+
+    @classmethod
+    def build(cls, ctx: Context, model: Model, rates: np.ndarray) -> "Net":
+        rates = np.ascontiguousarray(rates, np.float64)
+        h = C.c_void_p()
+        check(lib().esl_net_build(ctx._h, model._h, _ptr(rates), C.byref(h)))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_csc(cls, ctx: Context, n: int, indptr, rows) -> "Net":
+        h = C.c_void_p()
+        check(lib().esl_net_from_csc(ctx._h, n, _ptr(indptr), _ptr(rows), C.byref(h)))
+        return cls(ctx, h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.esl_net_free(self._h)
+            self._h = None
+
+    def export(self):
+        torch = _torch()
+        dev = f"cuda:{self.ctx.device}"
+        order = torch.empty(self.N, dtype=torch.int32, device=dev)
+        offsets = torch.empty(self.n_sccs + 1, dtype=torch.int32, device=dev)
+        levels = torch.empty(max(self.n_sccs, 1), dtype=torch.int32, device=dev)
+        labels = torch.empty(self.N, dtype=torch.int32, device=dev)
+        check(lib().esl_net_export(self.ctx._h, self._h, _ptr(order), _ptr(offsets), _ptr(levels), _ptr(labels)))
+        return order, offsets, levels[: self.n_sccs], labels
+
+    def compatible(self, rates: np.ndarray) -> bool:
+        rates = np.ascontiguousarray(rates, np.float64)
+        ok = C.c_int()
+        check(lib().esl_net_compatible(self._h, _ptr(rates), C.byref(ok)))
+        return bool(ok.value)
+
+
+@dataclass
+class SolveResult:
+    x_inf: object
+    marginals: object
+    R: object = None
+    L: object = None
+    report: Optional[Report] = None
+
+
+def _opts(method: int, tol: float, max_iters: int, max_refine: int, warm=None) -> SolveOpts:
+    return SolveOpts(method, tol, max_iters, max_refine, _ptr(warm))
+
+
+def solve(ctx: Context, net: Net, rates, x0, want_R: bool = False, want_L: bool = False,
+          method: int = METHOD_FP64, tol: float = 1e-10, max_iters: int = 0, max_refine: int = 0) -> SolveResult:
+    """One (rate set, x0): x_inf, marginals and optionally R (terminal kernels in
+    reordered position) and the dense absorption matrix L (T x N)."""
+    torch = _torch()
+    dev = f"cuda:{ctx.device}"
+    rates = torch.as_tensor(np.ascontiguousarray(rates, np.float64) if isinstance(rates, np.ndarray) else rates,
+                            dtype=torch.float64, device=dev).contiguous()
+    x0 = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
+    xi = torch.empty(net.N, dtype=torch.float64, device=dev)
+    mg = torch.empty(net.n, dtype=torch.float64, device=dev)
+    Rv = torch.empty(max(net.terminal_states, 1), dtype=torch.float64, device=dev) if want_R else None
+    Lm = torch.empty((net.T, net.N), dtype=torch.float64, device=dev) if want_L else None
+    rep = Report()
+    o = _opts(method, tol, max_iters, max_refine)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    check(lib().esl_solve(ctx._h, net._h, _ptr(rates), _ptr(x0), _ptr(xi), _ptr(mg), _ptr(Rv), _ptr(Lm),
+                          C.byref(o), C.byref(rep)))
+    return SolveResult(xi, mg, Rv[: net.terminal_states] if want_R else None, Lm, rep)
+
+
+def solve_batch(ctx: Context, net: Net, rates, x0, method: int = METHOD_FP64, tol: float = 1e-10,
+                max_iters: int = 0, max_refine: int = 0, warm=None, out=None, marginals: bool = True) -> SolveResult:
+    """B rate sets (B x 2n) x R initial distributions (R x N) -> x_inf (B x R x N)."""
+    torch = _torch()
+    dev = f"cuda:{ctx.device}"
+    rates = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
+    x0 = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
+    if rates.dim() == 1:
+        rates = rates[None]
+    if x0.dim() == 1:
+        x0 = x0[None]
+    B, R = rates.shape[0], x0.shape[0]
+    xi = out if out is not None else torch.empty((B, R, net.N), dtype=torch.float64, device=dev)
+    mg = torch.empty((B, R, net.n), dtype=torch.float64, device=dev) if marginals else None
+    rep = Report()
+    o = _opts(method, tol, max_iters, max_refine, warm)
+    check(lib().esl_solve_batch(ctx._h, net._h, B, _ptr(rates), R, _ptr(x0), _ptr(xi), _ptr(mg), C.byref(o),
+                                C.byref(rep)))
+    return SolveResult(xi, mg, report=rep)
+
+
+def solve_host(ctx: Context, model: Model, rates: np.ndarray, x0: np.ndarray, method: int = METHOD_FP64,
+               tol: float = 1e-10):
+    """Host arrays in, host arrays out (builds its own symbolic data)."""
+    rates = np.ascontiguousarray(np.atleast_2d(rates), np.float64)
+    x0 = np.ascontiguousarray(np.atleast_2d(x0), np.float64)
+    B, R = rates.shape[0], x0.shape[0]
+    N = 1 << model.n
+    xi = np.zeros((B, R, N))
+    mg = np.zeros((B, R, model.n))
+    rep = Report()
+    o = _opts(method, tol, 0, 0)
+    check(lib().esl_solve_host(ctx._h, model._h, B, _ptr(rates), R, _ptr(x0), _ptr(xi), _ptr(mg), C.byref(o),
+                               C.byref(rep)))
+    return xi, mg, rep

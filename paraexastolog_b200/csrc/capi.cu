@@ -1,0 +1,466 @@
+// C ABI of the library (declarations and reference citations in include/esl_b200.h).
+#include <cub/device/device_scan.cuh>
+
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+
+#include "esl_internal.h"
+
+namespace esl {
+
+static thread_local std::string g_error;
+
+void set_error(const std::string& msg) { g_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+namespace {
+
+__global__ void k_initial_state(uint64_t N, uint32_t fixed_mask, uint32_t fixed_val, double p_fixed,
+                                double p_other, double* __restrict__ x0) {
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    x0[s] = (((uint32_t)s & fixed_mask) == fixed_val) ? p_fixed : p_other;
+}
+
+int check_rates(const Model& m, const double* rates) {
+    if (!rates) return fail(ESL_ERR_INVALID, "rates is NULL");
+    for (int j = 0; j < 2 * m.n(); j++)
+        if (!(rates[j] >= 0.0) || !std::isfinite(rates[j]))
+            return fail(ESL_ERR_INVALID, "transition rate must be non-negative and finite");
+    return ESL_OK;
+}
+
+int rate_map(const Model& m, int count, const char* const* names, const double* vals, std::vector<int>& idx) {
+    idx.assign(m.n(), -1);
+    for (int k = 0; k < count; k++) {
+        int found = -1;
+        for (int i = 0; i < m.n(); i++)
+            if (m.names[i] == names[k]) {
+                found = i;
+                break;
+            }
+        if (found < 0) return fail(ESL_ERR_INVALID, std::string("node ") + names[k] + " not found");
+        if (vals[k] < 0) return fail(ESL_ERR_INVALID, "transition rate must be non-negative");
+        idx[found] = k;
+    }
+    return ESL_OK;
+}
+
+// Table counts: masks + per-block edge counts; returns nnz.
+int table_pass(esl_ctx* ctx, const Model& m, const double* rates, DevBuf<uint32_t>& F, DevBuf<uint32_t>& G,
+               DevBuf<uint32_t>& counts, int64_t& nnz, bool want_G) {
+    ESL_TRY(check_rates(m, rates));
+    cudaStream_t s = ctx->stream;
+    DevBuf<int32_t> off;
+    DevBuf<uint32_t> pos, neg;
+    DevModel dm;
+    ESL_TRY(upload_model(m, off, pos, neg, rates, dm, s));
+    const uint64_t N = 1ull << m.n();
+    ESL_TRY(F.alloc(N));
+    if (want_G) ESL_TRY(G.alloc(N));
+    const int64_t blocks = flip_mask_blocks(m.n());
+    ESL_TRY(counts.alloc(blocks + 1));
+    ESL_TRY(launch_flip_masks(dm, F.get(), want_G ? G.get() : nullptr, counts.get(), s));
+    std::vector<uint32_t> h(blocks);
+    ESL_CUDA(cudaMemcpyAsync(h.data(), counts.get(), blocks * 4, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    nnz = 0;
+    for (uint32_t c : h) nnz += c;
+    return ESL_OK;
+}
+
+}  // namespace
+}  // namespace esl
+
+using namespace esl;
+
+extern "C" {
+
+const char* esl_last_error(void) { return g_error.c_str(); }
+int esl_version(void) { return 100; }
+
+int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out) {
+    if (!out) return fail(ESL_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    ESL_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(ESL_ERR_INVALID, "no such CUDA device");
+    ESL_CUDA(cudaSetDevice(device));
+    auto* c = new esl_ctx();
+    c->device = device;
+    if (cuda_stream) {
+        c->stream = (cudaStream_t)cuda_stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return fail(ESL_ERR_CUDA, "cudaStreamCreate failed");
+        }
+        c->own_stream = true;
+    }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMallocHost(&c->h_flag, 64) != cudaSuccess || c->d_flag.alloc(8) != ESL_OK) {
+        esl_ctx_destroy(c);
+        return fail(ESL_ERR_NOMEM, "context allocation failed");
+    }
+    *out = c;
+    return ESL_OK;
+}
+
+int esl_ctx_destroy(esl_ctx* c) {
+    if (!c) return ESL_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->work) free_workspace(c->work);
+    c->d_flag.release();
+    if (c->h_flag) cudaFreeHost(c->h_flag);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ESL_OK;
+}
+
+int esl_ctx_synchronize(esl_ctx* c) {
+    if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
+    ESL_CUDA(cudaStreamSynchronize(c->stream));
+    return ESL_OK;
+}
+
+int esl_model_parse(const char* text, esl_model** out) {
+    if (!text || !out) return fail(ESL_ERR_INVALID, "NULL argument");
+    auto* m = new esl_model();
+    int st = parse_bnet(text, m->m);
+    if (st != ESL_OK) {
+        delete m;
+        *out = nullptr;
+        return st;
+    }
+    *out = m;
+    return ESL_OK;
+}
+
+int esl_model_load(const char* path, esl_model** out) {
+    if (!path || !out) return fail(ESL_ERR_INVALID, "NULL argument");
+    std::ifstream f(path, std::ios::binary);
+    if (!f.is_open()) return fail(ESL_ERR_INVALID, "could not open model file");
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return esl_model_parse(ss.str().c_str(), out);
+}
+
+int esl_model_free(esl_model* m) {
+    delete m;
+    return ESL_OK;
+}
+
+int esl_model_nodes(const esl_model* m, int* n) {
+    if (!m || !n) return fail(ESL_ERR_INVALID, "NULL argument");
+    *n = m->m.n();
+    return ESL_OK;
+}
+
+const char* esl_model_node_name(const esl_model* m, int i) {
+    if (!m || i < 0 || i >= m->m.n()) return nullptr;
+    return m->m.names[i].c_str();
+}
+
+int esl_model_node_index(const esl_model* m, const char* name, int* index) {
+    if (!m || !name || !index) return fail(ESL_ERR_INVALID, "NULL argument");
+    for (int i = 0; i < m->m.n(); i++)
+        if (m->m.names[i] == name) {
+            *index = i;
+            return ESL_OK;
+        }
+    return fail(ESL_ERR_INVALID, std::string("node ") + name + " not found");
+}
+
+int esl_model_clauses(const esl_model* m, int32_t* off, uint32_t* pos, uint32_t* neg, int cap, int* total) {
+    if (!m || !total) return fail(ESL_ERR_INVALID, "NULL argument");
+    int t = 0;
+    for (auto& r : m->m.rules) t += (int)r.size();
+    *total = t;
+    if (cap < t || !off || !pos || !neg) return ESL_OK;
+    int k = 0;
+    off[0] = 0;
+    for (int i = 0; i < m->m.n(); i++) {
+        for (auto& c : m->m.rules[i]) {
+            pos[k] = c.pos;
+            neg[k] = c.neg;
+            k++;
+        }
+        off[i + 1] = k;
+    }
+    return ESL_OK;
+}
+
+int esl_rates_uniform(const esl_model* m, int n_up, const char* const* up_names, const double* up_vals, int n_down,
+                      const char* const* down_names, const double* down_vals, double* rates_out) {
+    if (!m || !rates_out) return fail(ESL_ERR_INVALID, "NULL argument");
+    std::vector<int> ui, di;
+    ESL_TRY(rate_map(m->m, n_up, up_names, up_vals, ui));
+    ESL_TRY(rate_map(m->m, n_down, down_names, down_vals, di));
+    for (int i = 0; i < m->m.n(); i++) {
+        rates_out[2 * i] = ui[i] >= 0 ? up_vals[ui[i]] : 1.0;
+        rates_out[2 * i + 1] = di[i] >= 0 ? down_vals[di[i]] : 1.0;
+    }
+    return ESL_OK;
+}
+
+// Same generator as transition_rates::generate_normal (cuda/src/transition_rates.cpp:75-97):
+// std::default_random_engine (default-seeded when seed == 0) and a float normal
+// distribution, redrawing negatives up to 1000 times, node by node, up before down.
+int esl_rates_normal(const esl_model* m, double mean, double stddev, uint64_t seed, int n_up,
+                     const char* const* up_names, const double* up_vals, int n_down, const char* const* down_names,
+                     const double* down_vals, double* rates_out) {
+    if (!m || !rates_out) return fail(ESL_ERR_INVALID, "NULL argument");
+    std::vector<int> ui, di;
+    ESL_TRY(rate_map(m->m, n_up, up_names, up_vals, ui));
+    ESL_TRY(rate_map(m->m, n_down, down_names, down_vals, di));
+    std::default_random_engine gen;
+    if (seed) gen.seed((std::default_random_engine::result_type)seed);
+    std::normal_distribution<float> dist((float)mean, (float)stddev);
+    auto draw = [&](double& out) -> int {
+        float v;
+        int count = 0;
+        do {
+            v = dist(gen);
+            count++;
+        } while (v < 0 && count < 1000);
+        if (v < 0) return fail(ESL_ERR_INVALID, "could not generate positive transition rates with the provided mean and std");
+        out = v;
+        return ESL_OK;
+    };
+    for (int i = 0; i < m->m.n(); i++) {
+        if (ui[i] >= 0) rates_out[2 * i] = up_vals[ui[i]];
+        else ESL_TRY(draw(rates_out[2 * i]));
+        if (di[i] >= 0) rates_out[2 * i + 1] = down_vals[di[i]];
+        else ESL_TRY(draw(rates_out[2 * i + 1]));
+    }
+    return ESL_OK;
+}
+
+int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char* const* fixed_names,
+                      const int* fixed_values, double fixed_probability, double* d_x0) {
+    if (!ctx || !m || !d_x0 || (n_fixed > 0 && (!fixed_names || !fixed_values)))
+        return fail(ESL_ERR_INVALID, "NULL argument");
+    const int n = m->m.n();
+    const uint64_t N = 1ull << n;
+    uint32_t mask = 0, val = 0;
+    for (int k = 0; k < n_fixed; k++) {
+        int idx = -1;
+        for (int i = 0; i < n; i++)
+            if (m->m.names[i] == fixed_names[k]) {
+                idx = i;
+                break;
+            }
+        if (idx < 0) return fail(ESL_ERR_INVALID, std::string("invalid initial node name: ") + fixed_names[k]);
+        mask |= 1u << idx;
+        if (fixed_values[k]) val |= 1u << idx;
+    }
+    double p_fixed, p_other;
+    if (n_fixed == 0) {
+        p_fixed = p_other = 1.0 / (double)N;
+    } else {
+        uint64_t match = N >> __builtin_popcount(mask);
+        p_fixed = fixed_probability / (double)match;
+        p_other = match == N ? 0.0 : (1.0 - fixed_probability) / (double)(N - match);
+    }
+    k_initial_state<<<(unsigned)((N + 255) / 256), 256, 0, ctx->stream>>>(N, mask, val, p_fixed, p_other, d_x0);
+    ESL_CUDA(cudaGetLastError());
+    return ESL_OK;
+}
+
+int esl_table_nnz(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* nnz) {
+    if (!ctx || !m || !nnz) return fail(ESL_ERR_INVALID, "NULL argument");
+    DevBuf<uint32_t> F, G, counts;
+    ESL_TRY(table_pass(ctx, m->m, rates, F, G, counts, *nnz, false));
+    return ESL_OK;
+}
+
+int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32_t* d_indptr, int32_t* d_rows,
+                    int32_t* d_cols) {
+    if (!ctx || !m || !d_indptr || !d_rows) return fail(ESL_ERR_INVALID, "NULL argument");
+    DevBuf<uint32_t> F, G, counts;
+    int64_t nnz = 0;
+    ESL_TRY(table_pass(ctx, m->m, rates, F, G, counts, nnz, false));
+    if (nnz >= (int64_t)INT32_MAX) return fail(ESL_ERR_TOO_LARGE, "more than 2^31-1 transitions");
+    const int64_t blocks = flip_mask_blocks(m->m.n());
+    DevBuf<uint32_t> offs;
+    ESL_TRY(offs.alloc(blocks));
+    size_t tmp = 0;
+    ESL_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, counts.get(), offs.get(), (int)blocks, ctx->stream));
+    DevBuf<uint8_t> tbuf;
+    ESL_TRY(tbuf.alloc(tmp));
+    ESL_CUDA(cub::DeviceScan::ExclusiveSum(tbuf.get(), tmp, counts.get(), offs.get(), (int)blocks, ctx->stream));
+    ESL_TRY(launch_emit_csc(m->m.n(), F.get(), offs.get(), d_indptr, d_rows, d_cols, nnz, ctx->stream));
+    ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ESL_OK;
+}
+
+int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in) {
+    if (!ctx || !m || !d_out) return fail(ESL_ERR_INVALID, "NULL argument");
+    ESL_TRY(check_rates(m->m, rates));
+    DevBuf<int32_t> off;
+    DevBuf<uint32_t> pos, neg;
+    DevModel dm;
+    ESL_TRY(upload_model(m->m, off, pos, neg, rates, dm, ctx->stream));
+    ESL_TRY(launch_flip_masks(dm, d_out, d_in, nullptr, ctx->stream));
+    ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ESL_OK;
+}
+
+int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net** out) {
+    if (!ctx || !m || !out) return fail(ESL_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    auto* net = new esl_net();
+    net->n = m->m.n();
+    net->N = 1ll << net->n;
+    for (int i = 0; i < net->n; i++) {
+        if (rates[2 * i] != 0.0) net->up_ok |= 1u << i;
+        if (rates[2 * i + 1] != 0.0) net->down_ok |= 1u << i;
+    }
+    DevBuf<uint32_t> counts;
+    int64_t nnz = 0;
+    int st = table_pass(ctx, m->m, rates, net->F, net->G, counts, nnz, true);
+    if (st == ESL_OK) st = build_graph(ctx, net);
+    if (st != ESL_OK) {
+        delete net;
+        return st;
+    }
+    *out = net;
+    return ESL_OK;
+}
+
+int esl_net_from_csc(esl_ctx* ctx, int n_nodes, const int32_t* d_indptr, const int32_t* d_rows, esl_net** out) {
+    if (!ctx || !d_indptr || !d_rows || !out) return fail(ESL_ERR_INVALID, "NULL argument");
+    if (n_nodes < 1 || n_nodes > ESL_MAX_NODES) return fail(ESL_ERR_INVALID, "node count out of range");
+    *out = nullptr;
+    auto* net = new esl_net();
+    net->n = n_nodes;
+    net->N = 1ll << n_nodes;
+    net->up_ok = net->down_ok = (n_nodes >= 32) ? ~0u : ((1u << n_nodes) - 1);
+    int st = net->F.alloc(net->N);
+    if (st == ESL_OK) st = net->G.alloc(net->N);
+    if (st == ESL_OK) {
+        ESL_CUDA(cudaMemsetAsync(ctx->d_flag.get(), 0, 8, ctx->stream));
+        st = masks_from_csc(n_nodes, d_indptr, d_rows, net->F.get(), net->G.get(), ctx->d_flag.get(), ctx->stream);
+    }
+    if (st == ESL_OK) {
+        unsigned long long bad = 0;
+        ESL_CUDA(cudaMemcpyAsync(&bad, ctx->d_flag.get(), 8, cudaMemcpyDeviceToHost, ctx->stream));
+        ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (bad) st = fail(ESL_ERR_INVALID, "table has edges that do not flip exactly one bit");
+    }
+    if (st == ESL_OK) st = build_graph(ctx, net);
+    if (st != ESL_OK) {
+        delete net;
+        return st;
+    }
+    *out = net;
+    return ESL_OK;
+}
+
+int esl_net_free(esl_net* net) {
+    delete net;
+    return ESL_OK;
+}
+
+int esl_net_info(const esl_net* net, int* n_nodes, int* n_sccs, int* n_terminals, int* n_terminal_states) {
+    if (!net) return fail(ESL_ERR_INVALID, "net is NULL");
+    if (n_nodes) *n_nodes = net->n;
+    if (n_sccs) *n_sccs = net->n_sccs;
+    if (n_terminals) *n_terminals = net->T;
+    if (n_terminal_states) *n_terminal_states = net->term_states;
+    return ESL_OK;
+}
+
+int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* d_offsets, int32_t* d_levels,
+                   int32_t* d_labels) {
+    if (!ctx || !net) return fail(ESL_ERR_INVALID, "NULL argument");
+    cudaStream_t s = ctx->stream;
+    if (d_order) ESL_CUDA(cudaMemcpyAsync(d_order, net->order.get(), net->N * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_offsets)
+        ESL_CUDA(cudaMemcpyAsync(d_offsets, net->offsets.get(), (net->n_sccs + 1) * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_levels) ESL_CUDA(cudaMemcpyAsync(d_levels, net->levels.get(), net->n_sccs * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_labels) ESL_CUDA(cudaMemcpyAsync(d_labels, net->labels.get(), net->N * 4, cudaMemcpyDeviceToDevice, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    return ESL_OK;
+}
+
+int esl_net_compatible(const esl_net* net, const double* rates, int* compatible) {
+    if (!net || !rates || !compatible) return fail(ESL_ERR_INVALID, "NULL argument");
+    uint32_t up = 0, down = 0;
+    for (int i = 0; i < net->n; i++) {
+        if (rates[2 * i] != 0.0) up |= 1u << i;
+        if (rates[2 * i + 1] != 0.0) down |= 1u << i;
+    }
+    *compatible = (up == net->up_ok && down == net->down_ok) ? 1 : 0;
+    return ESL_OK;
+}
+
+static int check_batch_rates(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates) {
+    std::vector<double> h((size_t)B * 2 * net->n);
+    ESL_CUDA(cudaMemcpyAsync(h.data(), d_rates, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int b = 0; b < B; b++) {
+        const double* r = h.data() + (size_t)b * 2 * net->n;
+        for (int j = 0; j < 2 * net->n; j++)
+            if (!(r[j] >= 0.0) || !std::isfinite(r[j]))
+                return fail(ESL_ERR_INVALID, "rate set " + std::to_string(b) + " has a negative or non-finite rate");
+        int ok = 0;
+        esl_net_compatible(net, r, &ok);
+        if (!ok)
+            return fail(ESL_ERR_INVALID,
+                        "rate set " + std::to_string(b) + " has a different zero pattern than the network was built for");
+    }
+    return ESL_OK;
+}
+
+int esl_solve(esl_ctx* ctx, const esl_net* net, const double* d_rates, const double* d_x0, double* d_x_inf,
+              double* d_marginals, double* d_R, double* d_L, const esl_solve_opts* opts, esl_report* report) {
+    if (!ctx || !net || !d_rates || !d_x0) return fail(ESL_ERR_INVALID, "NULL argument");
+    ESL_TRY(check_batch_rates(ctx, net, 1, d_rates));
+    return solve_batch(ctx, net, 1, d_rates, 1, d_x0, d_x_inf, d_marginals, d_R, d_L, opts, report);
+}
+
+int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
+                    double* d_x_inf, double* d_marginals, const esl_solve_opts* opts, esl_report* report) {
+    if (!ctx || !net || !d_rates || !d_x0) return fail(ESL_ERR_INVALID, "NULL argument");
+    if (B < 1 || R < 1 || (int64_t)B * R > 65535) return fail(ESL_ERR_INVALID, "B*R must be in [1, 65535]");
+    ESL_TRY(check_batch_rates(ctx, net, B, d_rates));
+    return solve_batch(ctx, net, B, d_rates, R, d_x0, d_x_inf, d_marginals, nullptr, nullptr, opts, report);
+}
+
+int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,
+                   double* x_inf, double* marginals, const esl_solve_opts* opts, esl_report* report) {
+    if (!ctx || !m || !rates || !x0 || !x_inf) return fail(ESL_ERR_INVALID, "NULL argument");
+    if (B < 1 || R < 1) return fail(ESL_ERR_INVALID, "B and R must be positive");
+    const int n = m->m.n();
+    const size_t N = (size_t)1 << n;
+    cudaStream_t s = ctx->stream;
+    esl_net* net = nullptr;
+    ESL_TRY(esl_net_build(ctx, m, rates, &net));
+    DevBuf<double> dr, dx0, dxi, dm;
+    int st = dr.alloc((size_t)B * 2 * n);
+    if (st == ESL_OK) st = dx0.alloc((size_t)R * N);
+    if (st == ESL_OK) st = dxi.alloc((size_t)B * R * N);
+    if (st == ESL_OK && marginals) st = dm.alloc((size_t)B * R * n);
+    if (st == ESL_OK) {
+        cudaMemcpyAsync(dr.get(), rates, (size_t)B * 2 * n * 8, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dx0.get(), x0, (size_t)R * N * 8, cudaMemcpyHostToDevice, s);
+        st = esl_solve_batch(ctx, net, B, dr.get(), R, dx0.get(), dxi.get(), marginals ? dm.get() : nullptr, opts,
+                             report);
+    }
+    if (st == ESL_OK) {
+        cudaMemcpyAsync(x_inf, dxi.get(), (size_t)B * R * N * 8, cudaMemcpyDeviceToHost, s);
+        if (marginals) cudaMemcpyAsync(marginals, dm.get(), (size_t)B * R * n * 8, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(ESL_ERR_CUDA, "copy back failed");
+    }
+    esl_net_free(net);
+    return st;
+}
+
+}  // extern "C"

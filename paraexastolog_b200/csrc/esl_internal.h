@@ -1,0 +1,134 @@
+// Internal declarations shared by the ExaStoLog B200 library sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "esl_b200.h"
+
+namespace esl {
+
+// ---- errors ---------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define ESL_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::esl::fail(ESL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define ESL_TRY(call)                  \
+    do {                               \
+        int s_ = (call);               \
+        if (s_ != ESL_OK) return s_;   \
+    } while (0)
+
+// ---- host model -------------------------------------------------------------
+struct Clause {
+    uint32_t pos, neg;
+};
+
+struct Model {
+    std::vector<std::string> names;
+    std::vector<std::vector<Clause>> rules;
+    int n() const { return (int)names.size(); }
+};
+
+int parse_bnet(const std::string& text, Model& out);
+
+// ---- device buffers -----------------------------------------------------------
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(ESL_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        n = count;
+        return ESL_OK;
+    }
+    T* get() const { return p; }
+};
+
+}  // namespace esl
+
+// ---- public handles -------------------------------------------------------------
+struct esl_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+    uint32_t* h_flag = nullptr;       // pinned host scratch for fixpoint flags
+    esl::DevBuf<unsigned long long> d_flag;  // device counters (8 slots)
+    void* work = nullptr;             // solver workspace (grow-only), freed with the context
+};
+
+struct esl_model {
+    esl::Model m;
+};
+
+struct esl_net {
+    int n = 0;
+    int64_t N = 0;
+    uint32_t up_ok = 0, down_ok = 0;  // zero-rate pattern the net was built for
+    int n_sccs = 0, T = 0, term_states = 0;
+    esl::DevBuf<uint32_t> F, G;       // out / in flip masks
+    esl::DevBuf<int32_t> labels;      // SCC label (min vertex) per state
+    esl::DevBuf<int32_t> order;       // reordered vertices
+    esl::DevBuf<int32_t> offsets;     // SCC offsets in order (n_sccs + 1)
+    esl::DevBuf<int32_t> levels;      // level of the SCC at each offset position
+    esl::DevBuf<int32_t> term_of;     // terminal SCC index per state, -1 if transient
+    std::vector<int32_t> h_offsets;   // host copy of the terminal part of offsets (T + 1)
+    esl::DevBuf<uint32_t> Gdom;       // in-mask restricted to same-class neighbours
+    esl::DevBuf<uint32_t> Fdom;       // out-mask restricted to same-class neighbours
+    int max_terminal = 0;             // largest terminal SCC
+};
+
+namespace esl {
+
+// table.cu
+struct DevModel {
+    int n;
+    const int32_t* off;
+    const uint32_t* pos;
+    const uint32_t* neg;
+    uint32_t up_ok, down_ok, self_dep;
+};
+int upload_model(const Model& m, DevBuf<int32_t>& off, DevBuf<uint32_t>& pos, DevBuf<uint32_t>& neg,
+                 const double* rates, DevModel& dm, cudaStream_t s);
+int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* block_counts, cudaStream_t s);
+int64_t flip_mask_blocks(int n);
+int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
+                    int32_t* cols, int64_t nnz, cudaStream_t s);
+int masks_from_csc(int n, const int32_t* indptr, const int32_t* rows, uint32_t* F, uint32_t* G,
+                   unsigned long long* d_bad, cudaStream_t s);
+
+// graph.cu
+int build_graph(esl_ctx* ctx, esl_net* net);
+
+// solve.cu
+void free_workspace(void* w);
+int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
+                double* d_x_inf, double* d_marg, double* d_R, double* d_L, const esl_solve_opts* opts,
+                esl_report* rep);
+
+}  // namespace esl

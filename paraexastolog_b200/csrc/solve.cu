@@ -1,0 +1,1095 @@
+// Numeric phase: terminal kernels R, transient absorption, x_inf = R (L x0) and
+// per-node marginals, batched over rate sets and initial distributions.
+//
+// Replaces solver::solve (cuda/src/solver.cu:311-334): solve_terminal_part
+// (:102-159, minor determinants per state), solve_nonterminal_part (:205-300,
+// block LU of N^T with one triangular solve per terminal) and compute_final_states
+// (:302-309).
+//
+// Generator convention of the reference (cuda/src/kernels/solver.cu:20-44):
+// K[dst,src] = rate of src -> dst, rate index 2*i + (up ? 0 : 1) for a flip of bit i,
+// diagonal = -(total out-rate).
+//
+// Terminal kernels: per terminal SCC C, K_C pi = 0 with the last equation replaced
+// by sum(pi) = 1, dense FP64 LU with partial pivoting in shared memory (one CTA per
+// SCC and rate set); larger SCCs pin their first state and solve the remaining
+// (nonsingular) system with the Krylov engine below.
+//
+// Transient part, forward form (one system per rate set and x0): the expected
+// occupation z of the transient states solves (Q - A) z = x0 with Q = diag(out-rate)
+// and A the transient->transient rates; the mass entering terminal t is
+// y_t = x0(t) + sum over edges u->v, u transient, v in t of rate * z_u.  Backward
+// form (one system per rate set and terminal, gives the reference's L): h_t solves
+// (Q - A^T) h = rate into t.
+//
+// Every state-transition edge flips one bit, so the graph is bipartite by the parity
+// of popcount(state).  The systems are reduced to their odd-parity half (Schur
+// complement after eliminating the even half, whose diagonal block is diagonal);
+// half index h of state s is s >> 1.  The reduced system is solved by BiCGStab with
+// the Schur diagonal as (right) Jacobi preconditioner, inside an FP64 iterative
+// refinement loop: the true residual is always formed in FP64, the inner solve runs
+// in FP64 (ESL_METHOD_FP64) or FP32 (ESL_METHOD_MIXED).  All operators are applied
+// matrix-free from the flip masks and the rates.
+#include <cstdio>
+#include <cstring>
+
+#include "esl_internal.h"
+
+namespace esl {
+namespace {
+
+constexpr int kT = 256;
+constexpr uint32_t kDomainBit = 0x80000000u;
+constexpr uint32_t kMaskBits = 0x3FFFFFFFu;
+
+__device__ __forceinline__ uint32_t state_of(uint32_t h, int parity) {
+    return (h << 1) | (uint32_t)((__popc(h) & 1) ^ parity);
+}
+__device__ __forceinline__ uint32_t nb_half(uint32_t h, int i) { return i == 0 ? h : (h ^ (1u << (i - 1))); }
+
+// per-system scalar state of BiCGStab
+struct KState {
+    double rho, alpha, omega, beta;
+    double r0v, ts, tt, r0r, rr;
+    double rnorm2_true, bnorm2, target2;
+    int done, iters, breakdown, pad;
+};
+
+template <class T>
+__device__ __forceinline__ void load_rates(T* s_rate, const double* __restrict__ rates, int b, int n) {
+    for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) s_rate[j] = (T)rates[(size_t)b * 2 * n + j];
+}
+
+template <class T>
+__device__ __forceinline__ T out_rate(const T* s_rate, uint32_t f, uint32_t v) {
+    T q = 0;
+    while (f) {
+        int i = __ffs(f) - 1;
+        f &= f - 1;
+        q += s_rate[2 * i + ((v >> i) & 1u)];
+    }
+    return q;
+}
+
+// coupling of state v with its neighbour across bit i in v's equation
+template <bool FWD, class T>
+__device__ __forceinline__ T coupling(const T* s_rate, int i, uint32_t v) {
+    uint32_t bit = (v >> i) & 1u;
+    return FWD ? s_rate[2 * i + (bit ^ 1u)] : s_rate[2 * i + bit];
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// block-wide sum of up to 2 values, atomically added to dst0/dst1 by thread 0
+__device__ __forceinline__ void block_sum2(double a, double b, double* dst0, double* dst1) {
+    __shared__ double s_a[kT / 32], s_b[kT / 32];
+    a = warp_sum(a);
+    b = warp_sum(b);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        s_a[w] = a;
+        s_b[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < (int)(blockDim.x >> 5) ? s_a[l] : 0.0;
+        b = l < (int)(blockDim.x >> 5) ? s_b[l] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (l == 0) {
+            if (dst0) atomicAdd(dst0, a);
+            if (dst1) atomicAdd(dst1, b);
+        }
+    }
+}
+
+struct Layout {
+    int n;
+    uint32_t H;         // half length N/2
+    size_t ld;          // leading dimension of per-system vectors
+    int nrhs;           // systems per rate set
+    const uint32_t* M0; // even-half coupling masks | domain bit
+    const uint32_t* M1; // odd-half coupling masks | domain bit
+    const uint32_t* F0; // even-half out-masks
+    const uint32_t* F1; // odd-half out-masks
+};
+
+// wE[h] = (bE[h] + sum_i c_i x1[nb]) / q  on the even half (bE may be null)
+template <bool FWD, class T, class TX>
+__global__ void __launch_bounds__(kT) k_elim(Layout L, const double* __restrict__ rates, const TX* __restrict__ x1,
+                                             const double* __restrict__ bE, T* __restrict__ wE,
+                                             const KState* __restrict__ st) {
+    __shared__ T s_rate[64];
+    const int k = blockIdx.y;
+    if (st && st[k].done) return;
+    load_rates(s_rate, rates, k / L.nrhs, L.n);
+    __syncthreads();
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    const size_t o = (size_t)k * L.ld;
+    uint32_t m = L.M0[h];
+    if (!(m & kDomainBit)) {
+        wE[o + h] = 0;
+        return;
+    }
+    uint32_t v = state_of(h, 0);
+    T acc = bE ? (T)bE[o + h] : (T)0;
+    if (x1) {
+        uint32_t mm = m & kMaskBits;
+        while (mm) {
+            int i = __ffs(mm) - 1;
+            mm &= mm - 1;
+            acc += coupling<FWD>(s_rate, i, v) * (T)x1[o + nb_half(h, i)];
+        }
+    }
+    wE[o + h] = acc / out_rate(s_rate, L.F0[h], v);
+}
+
+// Odd-half operator.  mode 0: y = S x (and dot r0.y -> st.r0v);
+// mode 2: y = S x with x = s / dS, dots (y . dS x) -> ts and (y . y) -> tt;
+// mode 3: residual r = b - S x (FP64) with r.r -> rnorm2_true;
+// mode 4: rhs  y = b + sum_i c_i w[nb]  (x unused).
+template <bool FWD, int MODE, class T, class TX>
+__global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict__ rates, const TX* __restrict__ x,
+                                              const T* __restrict__ wE, const double* __restrict__ dS,
+                                              const double* __restrict__ b, const T* __restrict__ r0,
+                                              T* __restrict__ y, KState* __restrict__ st) {
+    __shared__ T s_rate[64];
+    const int k = blockIdx.y;
+    if (st && MODE != 3 && MODE != 4 && st[k].done) return;
+    load_rates(s_rate, rates, k / L.nrhs, L.n);
+    __syncthreads();
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    const size_t o = (size_t)k * L.ld;
+    double d0 = 0, d1 = 0;
+    if (h < L.H) {
+        uint32_t m = L.M1[h];
+        T out;
+        if (!(m & kDomainBit)) {
+            out = MODE == 4 ? (T)0 : (MODE == 3 ? (T)0 : (T)x[o + h]);
+        } else {
+            uint32_t v = state_of(h, 1);
+            T acc = 0;
+            uint32_t mm = m & kMaskBits;
+            while (mm) {
+                int i = __ffs(mm) - 1;
+                mm &= mm - 1;
+                acc += coupling<FWD>(s_rate, i, v) * wE[o + nb_half(h, i)];
+            }
+            if (MODE == 4) {
+                out = (T)b[o + h] + acc;
+            } else {
+                T q = out_rate(s_rate, L.F1[h], v);
+                T sx = q * (T)x[o + h] - acc;
+                out = MODE == 3 ? (T)b[o + h] - sx : sx;
+            }
+        }
+        y[o + h] = out;
+        if (MODE == 0) d0 = (double)r0[o + h] * (double)out;
+        if (MODE == 2) {
+            d0 = (double)out * (double)x[o + h] * dS[o + h];
+            d1 = (double)out * (double)out;
+        }
+        if (MODE == 3) d0 = (double)out * (double)out;
+    }
+    if (MODE == 0) block_sum2(d0, 0.0, &st[k].r0v, nullptr);
+    if (MODE == 2) block_sum2(d0, d1, &st[k].ts, &st[k].tt);
+    if (MODE == 3) block_sum2(d0, 0.0, &st[k].rnorm2_true, nullptr);
+}
+
+// Schur diagonal dS[h] = q_o - sum_i c_i(o) c_i(e)/q_e over odd states o (1 outside the domain)
+template <bool FWD>
+__global__ void __launch_bounds__(kT) k_schur_diag(Layout L, const double* __restrict__ rates, double* __restrict__ dS) {
+    __shared__ double s_rate[64];
+    const int k = blockIdx.y;
+    load_rates(s_rate, rates, k / L.nrhs, L.n);
+    __syncthreads();
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    const size_t o = (size_t)k * L.ld;
+    uint32_t m = L.M1[h];
+    if (!(m & kDomainBit)) {
+        dS[o + h] = 1.0;
+        return;
+    }
+    uint32_t v = state_of(h, 1);
+    double d = out_rate(s_rate, L.F1[h], v);
+    uint32_t mm = m & kMaskBits;
+    while (mm) {
+        int i = __ffs(mm) - 1;
+        mm &= mm - 1;
+        uint32_t he = nb_half(h, i);
+        uint32_t me = L.M0[he];
+        if ((me >> i) & 1u) {
+            uint32_t e = state_of(he, 0);
+            d -= coupling<FWD>(s_rate, i, v) * coupling<FWD>(s_rate, i, e) / out_rate(s_rate, L.F0[he], e);
+        }
+    }
+    dS[o + h] = d;
+}
+
+// ---- BiCGStab vector updates ------------------------------------------------------
+// start of an inner solve: r = r0 = (T) r64, d = 0, p = v = 0, scalars reset
+template <class T>
+__global__ void k_inner_start(Layout L, const double* __restrict__ r64, T* __restrict__ r, T* __restrict__ r0,
+                              T* __restrict__ d, T* __restrict__ ph, T* __restrict__ v, const KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].done) return;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    size_t i = (size_t)k * L.ld + h;
+    T val = (T)r64[i];
+    r[i] = val;
+    r0[i] = val;
+    d[i] = 0;
+    ph[i] = 0;
+    v[i] = 0;
+}
+
+template <class T>
+__global__ void k_update_p(Layout L, const double* __restrict__ dS, const T* __restrict__ r, T* __restrict__ ph,
+                           const T* __restrict__ v, const KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].done) return;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    size_t i = (size_t)k * L.ld + h;
+    T beta = (T)st[k].beta, omega = (T)st[k].omega;
+    T inv = (T)(1.0 / dS[i]);
+    ph[i] = r[i] * inv + beta * (ph[i] - omega * v[i] * inv);
+}
+
+template <class T>
+__global__ void k_update_s(Layout L, const double* __restrict__ dS, const T* __restrict__ r, const T* __restrict__ v,
+                           T* __restrict__ sh, const KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].done) return;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    size_t i = (size_t)k * L.ld + h;
+    T alpha = (T)st[k].alpha;
+    sh[i] = (r[i] - alpha * v[i]) * (T)(1.0 / dS[i]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT) k_update_xr(Layout L, const double* __restrict__ dS, T* __restrict__ d,
+                                                  T* __restrict__ r, const T* __restrict__ r0,
+                                                  const T* __restrict__ ph, const T* __restrict__ sh,
+                                                  const T* __restrict__ t, KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].done) return;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    double a = 0, b = 0;
+    if (h < L.H) {
+        size_t i = (size_t)k * L.ld + h;
+        T alpha = (T)st[k].alpha, omega = (T)st[k].omega;
+        d[i] += alpha * ph[i] + omega * sh[i];
+        T rn = (T)dS[i] * sh[i] - omega * t[i];
+        r[i] = rn;
+        a = (double)r0[i] * (double)rn;
+        b = (double)rn * (double)rn;
+    }
+    block_sum2(a, b, &st[k].r0r, &st[k].rr);
+}
+
+// scalar steps, one thread per system
+__global__ void k_scal_alpha(int K, KState* st) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K || st[k].done) return;
+    KState& s = st[k];
+    if (s.r0v == 0.0 || !isfinite(s.r0v)) {
+        s.breakdown = 1;
+        s.done = 1;
+        return;
+    }
+    s.alpha = s.rho / s.r0v;
+    s.ts = s.tt = 0.0;
+}
+
+__global__ void k_scal_omega(int K, KState* st) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K || st[k].done) return;
+    KState& s = st[k];
+    s.omega = s.tt > 0.0 ? s.ts / s.tt : 0.0;
+    s.r0r = s.rr = 0.0;
+}
+
+__global__ void k_scal_beta(int K, KState* st, int max_iters) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K || st[k].done) return;
+    KState& s = st[k];
+    s.iters++;
+    if (s.rr <= s.target2 || s.iters >= max_iters) {
+        s.done = 1;
+        return;
+    }
+    if (s.omega == 0.0 || s.r0r == 0.0 || !isfinite(s.r0r)) {
+        s.breakdown = 1;
+        s.done = 1;
+        return;
+    }
+    s.beta = (s.r0r / s.rho) * (s.alpha / s.omega);
+    s.rho = s.r0r;
+    s.r0v = 0.0;
+}
+
+// after the true residual: decide which systems still need an inner solve
+__global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2, int* n_active) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    KState& s = st[k];
+    bool conv = s.rnorm2_true <= tol2 * s.bnorm2 || s.bnorm2 == 0.0;
+    s.done = conv ? 1 : 0;
+    if (!conv) {
+        atomicAdd(n_active, 1);
+        s.rho = s.rnorm2_true;  // r0 = r at the start: rho = r0.r
+        s.alpha = s.omega = 1.0;
+        s.beta = 0.0;
+        s.r0v = 0.0;
+        // inner target: reach tol in one inner solve if the inner precision allows
+        s.target2 = fmax(0.25 * tol2 * s.bnorm2, inner_rel2 * s.rnorm2_true);
+        s.breakdown = 0;
+        s.iters = 0;
+    }
+}
+
+
+template <class T>
+__global__ void k_add_correction(Layout L, double* __restrict__ x64, const T* __restrict__ d,
+                                 const KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].pad) return;  // pad marks systems that had no inner solve this round
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    size_t i = (size_t)k * L.ld + h;
+    x64[i] += (double)d[i];
+}
+
+__global__ void k_mark_inner(int K, KState* st) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    st[k].pad = st[k].done;  // systems already converged get no correction
+}
+
+__global__ void k_zero_r(int K, KState* st) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    st[k].rnorm2_true = 0.0;
+}
+
+// ---- right-hand sides ---------------------------------------------------------------
+// forward: b = x0 on transient states; backward (system = (rate set, terminal t)):
+// b_v = sum of rates of edges v -> terminal t.  Written in both halves.
+template <bool FWD>
+__global__ void k_rhs(Layout L, int n, const double* __restrict__ rates, const double* __restrict__ x0,
+                      size_t x0_ld, const uint32_t* __restrict__ F, const int32_t* __restrict__ term_of,
+                      double* __restrict__ bE, double* __restrict__ bO) {
+    __shared__ double s_rate[64];
+    const int k = blockIdx.y;
+    load_rates(s_rate, rates, k / L.nrhs, L.n);
+    __syncthreads();
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    const size_t o = (size_t)k * L.ld;
+    const int r = k % L.nrhs;
+#pragma unroll
+    for (int par = 0; par < 2; par++) {
+        uint32_t v = state_of(h, par);
+        double val = 0.0;
+        if (term_of[v] < 0) {
+            if (FWD) {
+                val = x0[(size_t)r * x0_ld + v];
+            } else {
+                uint32_t f = F[v];
+                while (f) {
+                    int i = __ffs(f) - 1;
+                    f &= f - 1;
+                    if (term_of[v ^ (1u << i)] == r) val += s_rate[2 * i + ((v >> i) & 1u)];
+                }
+            }
+        }
+        (par ? bO : bE)[o + h] = val;
+    }
+}
+
+// ---- assembly ---------------------------------------------------------------------
+// forward: y[k][t] += x0(v) + sum_{u -> v, u transient} rate * z(u) over v in t
+__global__ void k_terminal_mass(int n, int T, int term_states, int nrhs, size_t ld, const double* __restrict__ rates,
+                                const double* __restrict__ x0, size_t x0_ld, const int32_t* __restrict__ order,
+                                const int32_t* __restrict__ term_of, const uint32_t* __restrict__ G,
+                                const double* __restrict__ zE, const double* __restrict__ zO,
+                                double* __restrict__ y) {
+    const int k = blockIdx.y;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= term_states) return;
+    const int b = k / nrhs, r = k % nrhs;
+    const double* rt = rates + (size_t)b * 2 * n;
+    uint32_t v = (uint32_t)order[p];
+    int t = term_of[v];
+    double acc = x0[(size_t)r * x0_ld + v];
+    uint32_t g = G[v];
+    while (g) {
+        int i = __ffs(g) - 1;
+        g &= g - 1;
+        uint32_t u = v ^ (1u << i);
+        if (term_of[u] >= 0) continue;
+        uint32_t hu = u >> 1;
+        double zu = (__popc(u) & 1) ? zO[(size_t)k * ld + hu] : zE[(size_t)k * ld + hu];
+        acc += rt[2 * i + ((u >> i) & 1u)] * zu;
+    }
+    atomicAdd(&y[(size_t)k * T + t], acc);
+}
+
+// x_inf[k][v] = R_b[pos] * y[k][t] on terminal states; marginals accumulated
+__global__ void k_scatter_xinf(int n, int T, int term_states, int nrhs, size_t N, const int32_t* __restrict__ order,
+                               const int32_t* __restrict__ term_of, const double* __restrict__ Rb,
+                               const double* __restrict__ y, double* __restrict__ x_inf, double* __restrict__ marg) {
+    const int k = blockIdx.y;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= term_states) return;
+    const int b = k / nrhs;
+    uint32_t v = (uint32_t)order[p];
+    int t = term_of[v];
+    double val = Rb[(size_t)b * term_states + p] * y[(size_t)k * T + t];
+    x_inf[(size_t)k * N + v] = val;
+    if (marg && val != 0.0) {
+        for (int i = 0; i < n; i++)
+            if ((v >> i) & 1u) atomicAdd(&marg[(size_t)k * n + i], val);
+    }
+}
+
+// ---- dense terminal kernels ----------------------------------------------------------
+// One CTA per (terminal SCC of size 2..kDenseTerm, rate set).  A = K_C with the last row
+// replaced by ones; solve A pi = e_last by Gaussian elimination with partial pivoting.
+constexpr int kDenseTerm = 128;
+
+__global__ void __launch_bounds__(256) k_dense_terminal(int n, const int32_t* __restrict__ sccs,
+                                                        const int32_t* __restrict__ offsets,
+                                                        const int32_t* __restrict__ order,
+                                                        const uint32_t* __restrict__ F,
+                                                        const double* __restrict__ rates, int term_states,
+                                                        double* __restrict__ Rb) {
+    extern __shared__ double s_mem[];
+    __shared__ double s_rate[64];
+    __shared__ int s_piv;
+    const int t = sccs[blockIdx.x];
+    const int b = blockIdx.y;
+    const int beg = offsets[t];
+    const int s = offsets[t + 1] - beg;
+    double* A = s_mem;                         // s x (s+1), last column = rhs
+    int32_t* mem = (int32_t*)(A + s * (s + 1));
+    const int ld = s + 1;
+    for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) s_rate[j] = rates[(size_t)b * 2 * n + j];
+    for (int j = threadIdx.x; j < s; j += blockDim.x) mem[j] = order[beg + j];
+    for (int j = threadIdx.x; j < s * ld; j += blockDim.x) A[j] = 0.0;
+    __syncthreads();
+    // column c = source state mem[c]; members are ascending, so locate by binary search
+    for (int c = threadIdx.x; c < s; c += blockDim.x) {
+        uint32_t v = (uint32_t)mem[c];
+        uint32_t f = F[v];
+        double diag = 0.0;
+        while (f) {
+            int i = __ffs(f) - 1;
+            f &= f - 1;
+            int32_t w = (int32_t)(v ^ (1u << i));
+            int lo = 0, hi = s - 1;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (mem[mid] < w) lo = mid + 1; else hi = mid;
+            }
+            double rt = s_rate[2 * i + ((v >> i) & 1u)];
+            if (mem[lo] == w && lo != s - 1) A[lo * ld + c] += rt;  // row lo, written only by column c
+            diag += rt;
+        }
+        if (c != s - 1) A[c * ld + c] -= diag;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < s; c += blockDim.x) A[(s - 1) * ld + c] = 1.0;
+    for (int r = threadIdx.x; r < s; r += blockDim.x) A[r * ld + s] = (r == s - 1) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int col = 0; col < s; col++) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = col;
+            for (int r = col + threadIdx.x; r < s; r += 32) {
+                double a = fabs(A[r * ld + col]);
+                if (a > best) { best = a; bi = r; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+                int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (threadIdx.x == 0) s_piv = bi;
+        }
+        __syncthreads();
+        const int piv = s_piv;
+        if (piv != col)
+            for (int j = col + threadIdx.x; j <= s; j += blockDim.x) {
+                double tmp = A[col * ld + j];
+                A[col * ld + j] = A[piv * ld + j];
+                A[piv * ld + j] = tmp;
+            }
+        __syncthreads();
+        const double inv = 1.0 / A[col * ld + col];
+        const int rows = s - col - 1, cols = s - col;  // columns col+1 .. s
+        for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
+            int r = col + 1 + e / cols, j = col + 1 + e % cols;
+            A[r * ld + j] -= A[r * ld + col] * inv * A[col * ld + j];
+        }
+        __syncthreads();
+    }
+    // back substitution on the rhs column (single warp, rows descending)
+    if (threadIdx.x < 32) {
+        for (int r = s - 1; r >= 0; r--) {
+            double acc = 0.0;
+            for (int j = r + 1 + threadIdx.x; j < s; j += 32) acc += A[r * ld + j] * A[j * ld + s];
+            acc = warp_sum(acc);
+            if (threadIdx.x == 0) A[r * ld + s] = (A[r * ld + s] - acc) / A[r * ld + r];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // normalise |pi| (the reference normalises |minor determinants| the same way)
+    if (threadIdx.x < 32) {
+        double sum = 0.0;
+        for (int j = threadIdx.x; j < s; j += 32) sum += fabs(A[j * ld + s]);
+        sum = warp_sum(sum);
+        for (int j = threadIdx.x; j < s; j += 32) Rb[(size_t)b * term_states + beg + j] = fabs(A[j * ld + s]) / sum;
+    }
+}
+
+__global__ void k_unit_terminals(int T, const int32_t* __restrict__ offsets, int term_states, double* __restrict__ Rb) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    if (offsets[t + 1] - offsets[t] == 1) Rb[(size_t)blockIdx.y * term_states + offsets[t]] = 1.0;
+}
+
+// half-layout masks for one domain; domain(v) decided by `dom`:
+// dom = 0: transient states; dom = 1: states of "big" terminal SCCs except their pinned state
+__global__ void k_half_masks(int n, uint32_t H, const uint32_t* __restrict__ Md, const uint32_t* __restrict__ F,
+                             const int32_t* __restrict__ term_of, const uint8_t* __restrict__ big_term,
+                             const uint8_t* __restrict__ is_pin, int dom, uint32_t* __restrict__ M0,
+                             uint32_t* __restrict__ M1, uint32_t* __restrict__ F0, uint32_t* __restrict__ F1) {
+    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= H) return;
+    for (int par = 0; par < 2; par++) {
+        uint32_t v = state_of(h, par);
+        int t = term_of[v];
+        bool in;
+        if (dom == 0) in = t < 0;
+        else in = t >= 0 && big_term[t] && !is_pin[v];
+        uint32_t m = Md[v];
+        if (dom == 1 && in) {
+            // neighbours that are the pinned state are not unknowns
+            uint32_t mm = m, keep = 0;
+            while (mm) {
+                int i = __ffs(mm) - 1;
+                mm &= mm - 1;
+                if (!is_pin[v ^ (1u << i)]) keep |= 1u << i;
+            }
+            m = keep;
+        }
+        (par ? M1 : M0)[h] = in ? (m | kDomainBit) : 0u;
+        (par ? F1 : F0)[h] = F[v];
+    }
+}
+
+// pinned terminal systems: rhs b_v = rate(pin -> v) for states v of a big terminal SCC
+__global__ void k_rhs_pinned(int n, uint32_t H, size_t ld, const double* __restrict__ rates,
+                             const uint32_t* __restrict__ G, const uint8_t* __restrict__ is_pin,
+                             const uint32_t* __restrict__ M0, const uint32_t* __restrict__ M1,
+                             double* __restrict__ bE, double* __restrict__ bO) {
+    __shared__ double s_rate[64];
+    const int k = blockIdx.y;
+    load_rates(s_rate, rates, k, n);
+    __syncthreads();
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= H) return;
+    for (int par = 0; par < 2; par++) {
+        uint32_t v = state_of(h, par);
+        uint32_t m = (par ? M1 : M0)[h];
+        double val = 0.0;
+        if (m & kDomainBit) {
+            uint32_t g = G[v];
+            while (g) {
+                int i = __ffs(g) - 1;
+                g &= g - 1;
+                uint32_t u = v ^ (1u << i);
+                if (is_pin[u]) val += s_rate[2 * i + ((u >> i) & 1u)];
+            }
+        }
+        (par ? bO : bE)[(size_t)k * ld + h] = val;
+    }
+}
+
+// R for big terminal SCCs from the pinned solution z (pin = 1), normalised per SCC
+__global__ void k_pinned_sum(int T, const int32_t* __restrict__ offsets, const int32_t* __restrict__ order,
+                             const uint8_t* __restrict__ big_term, const uint8_t* __restrict__ is_pin, size_t ld,
+                             const double* __restrict__ zE, const double* __restrict__ zO, int term_states,
+                             double* __restrict__ Rb, double* __restrict__ sums) {
+    const int b = blockIdx.y;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= term_states) return;
+    uint32_t v = (uint32_t)order[p];
+    int t = 0;
+    {
+        int lo = 0, hi = T;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) / 2;
+            if (offsets[mid] <= p) lo = mid; else hi = mid;
+        }
+        t = lo;
+    }
+    if (!big_term[t]) return;
+    double val = is_pin[v] ? 1.0 : fabs((__popc(v) & 1) ? zO[(size_t)b * ld + (v >> 1)] : zE[(size_t)b * ld + (v >> 1)]);
+    Rb[(size_t)b * term_states + p] = val;
+    atomicAdd(&sums[(size_t)b * T + t], val);
+}
+
+__global__ void k_pinned_norm(int T, const int32_t* __restrict__ offsets, const uint8_t* __restrict__ big_term,
+                              int term_states, double* __restrict__ Rb, const double* __restrict__ sums) {
+    const int b = blockIdx.y;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= term_states) return;
+    int lo = 0, hi = T;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (offsets[mid] <= p) lo = mid; else hi = mid;
+    }
+    if (!big_term[lo]) return;
+    Rb[(size_t)b * term_states + p] /= sums[(size_t)b * T + lo];
+}
+
+// absorption matrix L[t][v] (backward form, one rate set): h on transient states,
+// 1 on the states of t
+__global__ void k_scatter_L(uint32_t H, int T, size_t N, size_t ld, const int32_t* __restrict__ term_of,
+                            const double* __restrict__ zE, const double* __restrict__ zO, double* __restrict__ Lm) {
+    const int t = blockIdx.y;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= H) return;
+    for (int par = 0; par < 2; par++) {
+        uint32_t v = state_of(h, par);
+        int c = term_of[v];
+        double val = c < 0 ? (par ? zO : zE)[(size_t)t * ld + h] : (c == t ? 1.0 : 0.0);
+        Lm[(size_t)t * N + v] = val;
+    }
+}
+
+// ---- driver ---------------------------------------------------------------------------------
+__global__ void k_count_running(int K, const KState* st, int* n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K && !st[k].done) atomicAdd(n, 1);
+}
+
+__global__ void __launch_bounds__(kT) k_norm2(uint32_t H, size_t ld, const double* __restrict__ x, KState* st) {
+    const int k = blockIdx.y;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    double a = 0.0;
+    if (h < H) {
+        double v = x[(size_t)k * ld + h];
+        a = v * v;
+    }
+    block_sum2(a, 0.0, &st[k].bnorm2, nullptr);
+}
+
+__global__ void k_half_from_full(uint32_t H, size_t ld, const double* __restrict__ full, size_t full_ld,
+                                 const uint32_t* __restrict__ M1, double* __restrict__ x1) {
+    const int k = blockIdx.y;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= H) return;
+    x1[(size_t)k * ld + h] = (M1[h] & kDomainBit) ? full[(size_t)k * full_ld + state_of(h, 1)] : 0.0;
+}
+
+template <class T>
+struct InnerVecs {
+    T *r, *r0, *ph, *v, *sh, *t, *d, *w;
+};
+
+inline dim3 grid2(uint32_t H, int K) { return dim3((H + kT - 1) / kT, (unsigned)K); }
+
+template <bool FWD, class T>
+int inner_bicgstab(esl_ctx* ctx, const Layout& L, const double* rates, int K, const double* dS, const double* r64,
+                   KState* st, int* n_active, InnerVecs<T> iv, int max_iters, int* iters_out) {
+    cudaStream_t s = ctx->stream;
+    dim3 g = grid2(L.H, K);
+    unsigned sb = (unsigned)((K + 127) / 128);
+    k_inner_start<T><<<g, kT, 0, s>>>(L, r64, iv.r, iv.r0, iv.d, iv.ph, iv.v, st);
+    int it = 0;
+    const int check_every = 8;
+    while (it < max_iters) {
+        for (int c = 0; c < check_every; c++, it++) {
+            k_update_p<T><<<g, kT, 0, s>>>(L, dS, iv.r, iv.ph, iv.v, st);
+            k_elim<FWD, T, T><<<g, kT, 0, s>>>(L, rates, iv.ph, nullptr, iv.w, st);
+            k_apply<FWD, 0, T, T><<<g, kT, 0, s>>>(L, rates, iv.ph, iv.w, dS, nullptr, iv.r0, iv.v, st);
+            k_scal_alpha<<<sb, 128, 0, s>>>(K, st);
+            k_update_s<T><<<g, kT, 0, s>>>(L, dS, iv.r, iv.v, iv.sh, st);
+            k_elim<FWD, T, T><<<g, kT, 0, s>>>(L, rates, iv.sh, nullptr, iv.w, st);
+            k_apply<FWD, 2, T, T><<<g, kT, 0, s>>>(L, rates, iv.sh, iv.w, dS, nullptr, nullptr, iv.t, st);
+            k_scal_omega<<<sb, 128, 0, s>>>(K, st);
+            k_update_xr<T><<<g, kT, 0, s>>>(L, dS, iv.d, iv.r, iv.r0, iv.ph, iv.sh, iv.t, st);
+            k_scal_beta<<<sb, 128, 0, s>>>(K, st, max_iters);
+        }
+        ESL_CUDA(cudaGetLastError());
+        ESL_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s));
+        k_count_running<<<sb, 128, 0, s>>>(K, st, n_active);
+        int active = 0;
+        ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        if (active == 0) break;
+    }
+    *iters_out = it;
+    return ESL_OK;
+}
+
+}  // namespace
+
+// Grow-only device workspace kept in the context between calls.
+struct Workspace {
+    std::vector<std::pair<void*, size_t>> bufs;
+    void* get(int slot, size_t bytes, int* status) {
+        if ((int)bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
+        auto& b = bufs[slot];
+        if (b.second < bytes) {
+            if (b.first) cudaFree(b.first);
+            b.first = nullptr;
+            b.second = 0;
+            if (cudaMalloc(&b.first, bytes) != cudaSuccess) {
+                b.first = nullptr;
+                *status = fail(ESL_ERR_NOMEM, "workspace allocation of " + std::to_string(bytes) + " bytes failed");
+                return nullptr;
+            }
+            b.second = bytes;
+        }
+        return b.first;
+    }
+    ~Workspace() {
+        for (auto& b : bufs)
+            if (b.first) cudaFree(b.first);
+    }
+};
+
+void free_workspace(void* w) { delete static_cast<Workspace*>(w); }
+
+namespace {
+
+enum Slot {
+    S_BE, S_BS, S_DS, S_X64, S_R64, S_W64, S_ZE, S_ST, S_ACT,
+    S_R, S_R0, S_PH, S_V, S_SH, S_T, S_D, S_W,
+    S_M0, S_M1, S_F0, S_F1, S_RB, S_Y, S_SUM, S_BIG, S_PIN, S_BO, S_LIST, S_COUNT
+};
+
+struct SolveOut {
+    int iters = 0, refinements = 0;
+    double relres = 0.0;
+    bool converged = true;
+};
+
+// Solves the K systems whose rhs halves are in (bE, bO); solution in x64 (odd) and zE (even).
+template <bool FWD>
+int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rates, int K, double* bE, double* bO,
+                 const double* warm, size_t warm_ld, const esl_solve_opts& o, double*& x64_out, double*& zE_out,
+                 SolveOut& out) {
+    cudaStream_t s = ctx->stream;
+    int st_ = ESL_OK;
+    const size_t vec = (size_t)K * L.ld;
+    double* dS = (double*)ws.get(S_DS, vec * 8, &st_);
+    double* bS = (double*)ws.get(S_BS, vec * 8, &st_);
+    double* x64 = (double*)ws.get(S_X64, vec * 8, &st_);
+    double* r64 = (double*)ws.get(S_R64, vec * 8, &st_);
+    double* w64 = (double*)ws.get(S_W64, vec * 8, &st_);
+    double* zE = (double*)ws.get(S_ZE, vec * 8, &st_);
+    KState* st = (KState*)ws.get(S_ST, (size_t)K * sizeof(KState), &st_);
+    int* n_active = (int*)ws.get(S_ACT, sizeof(int), &st_);
+    const bool mixed = o.method == ESL_METHOD_MIXED;
+    const size_t tsz = mixed ? 4 : 8;
+    void* iv_p[8];
+    for (int j = 0; j < 8; j++) iv_p[j] = ws.get(S_R + j, vec * tsz, &st_);
+    if (st_ != ESL_OK) return st_;
+    dim3 g = grid2(L.H, K);
+    unsigned sb = (unsigned)((K + 127) / 128);
+    ESL_CUDA(cudaMemsetAsync(st, 0, (size_t)K * sizeof(KState), s));
+    k_schur_diag<FWD><<<g, kT, 0, s>>>(L, rates, dS);
+    // reduced rhs: bS = bO + A_oe (bE / q_e)
+    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, (const double*)nullptr, bE, w64, nullptr);
+    k_apply<FWD, 4, double, double><<<g, kT, 0, s>>>(L, rates, (const double*)nullptr, w64, dS, bO, nullptr, bS,
+                                                     nullptr);
+    k_norm2<<<g, kT, 0, s>>>(L.H, L.ld, bS, st);
+    if (warm)
+        k_half_from_full<<<g, kT, 0, s>>>(L.H, L.ld, warm, warm_ld, L.M1, x64);
+    else
+        ESL_CUDA(cudaMemsetAsync(x64, 0, vec * 8, s));
+    ESL_CUDA(cudaGetLastError());
+    const double tol = o.tol > 0 ? o.tol : 1e-10;
+    const double floor_rel = mixed ? 3e-6 : 1e-13;
+    int total_iters = 0, outer = 0;
+    int active = 0;
+    for (;; outer++) {
+        k_zero_r<<<sb, 128, 0, s>>>(K, st);
+        k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
+        k_apply<FWD, 3, double, double><<<g, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
+        ESL_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s));
+        // inner target: a relative reduction that reaches tol in one inner solve,
+        // but not below what the inner precision can deliver
+        k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_rel * floor_rel, n_active);
+        ESL_CUDA(cudaGetLastError());
+        ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        if (active == 0 || outer >= o.max_refine) break;
+        k_mark_inner<<<sb, 128, 0, s>>>(K, st);
+        int it = 0;
+        if (mixed) {
+            InnerVecs<float> iv{(float*)iv_p[0], (float*)iv_p[1], (float*)iv_p[2], (float*)iv_p[3],
+                                (float*)iv_p[4], (float*)iv_p[5], (float*)iv_p[6], (float*)iv_p[7]};
+            ESL_TRY((inner_bicgstab<FWD, float>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
+            k_add_correction<float><<<g, kT, 0, s>>>(L, x64, iv.d, st);
+        } else {
+            InnerVecs<double> iv{(double*)iv_p[0], (double*)iv_p[1], (double*)iv_p[2], (double*)iv_p[3],
+                                 (double*)iv_p[4], (double*)iv_p[5], (double*)iv_p[6], (double*)iv_p[7]};
+            ESL_TRY((inner_bicgstab<FWD, double>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
+            k_add_correction<double><<<g, kT, 0, s>>>(L, x64, iv.d, st);
+        }
+        ESL_CUDA(cudaGetLastError());
+        total_iters += it;
+    }
+    // even half: zE = (bE + A_eo x) / q_e
+    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, bE, zE, nullptr);
+    ESL_CUDA(cudaGetLastError());
+    std::vector<KState> h_st(K);
+    ESL_CUDA(cudaMemcpyAsync(h_st.data(), st, (size_t)K * sizeof(KState), cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    double worst = 0.0;
+    for (auto& k : h_st)
+        if (k.bnorm2 > 0) worst = std::max(worst, std::sqrt(k.rnorm2_true / k.bnorm2));
+    out.iters = total_iters;
+    out.refinements = outer;
+    out.relres = worst;
+    out.converged = active == 0;
+    x64_out = x64;
+    zE_out = zE;
+    if (!out.converged)
+        return fail(ESL_ERR_NOT_CONVERGED, "relative residual " + std::to_string(worst) + " above tolerance after " +
+                                               std::to_string(outer) + " refinement steps");
+    return ESL_OK;
+}
+
+int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const uint8_t* big_term,
+                const uint8_t* is_pin, bool fwd, Layout& L, int nrhs, int K) {
+    int st_ = ESL_OK;
+    const uint32_t H = (uint32_t)(net->N / 2);
+    uint32_t* M0 = (uint32_t*)ws.get(S_M0 + 0, (size_t)H * 4 * 4, &st_);
+    if (st_ != ESL_OK) return st_;
+    uint32_t* M1 = M0 + H;
+    uint32_t* F0 = M0 + 2 * (size_t)H;
+    uint32_t* F1 = M0 + 3 * (size_t)H;
+    k_half_masks<<<(H + kT - 1) / kT, kT, 0, ctx->stream>>>(net->n, H, fwd ? net->Gdom.get() : net->Fdom.get(),
+                                                           net->F.get(), net->term_of.get(), big_term, is_pin, dom, M0,
+                                                           M1, F0, F1);
+    ESL_CUDA(cudaGetLastError());
+    L.n = net->n;
+    L.H = H;
+    L.ld = ((size_t)H + 31) & ~(size_t)31;
+    L.nrhs = nrhs;
+    L.M0 = M0;
+    L.M1 = M1;
+    L.F0 = F0;
+    L.F1 = F1;
+    (void)K;
+    return ESL_OK;
+}
+
+}  // namespace
+
+int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
+                double* d_x_inf, double* d_marg, double* d_R, double* d_L, const esl_solve_opts* opts,
+                esl_report* rep) {
+    if (net->n < 1) return fail(ESL_ERR_INVALID, "network has no nodes");
+    esl_solve_opts o;
+    if (opts) o = *opts;
+    else {
+        o.method = ESL_METHOD_FP64;
+        o.tol = 0;
+        o.max_iters = 0;
+        o.max_refine = 0;
+        o.d_warm = nullptr;
+    }
+    if (o.tol <= 0) o.tol = 1e-10;
+    if (o.max_iters <= 0) o.max_iters = 2000;
+    if (o.max_refine <= 0) o.max_refine = 6;
+    if (o.method == ESL_METHOD_DIRECT)
+        return fail(ESL_ERR_INVALID, "ESL_METHOD_DIRECT is not available in this build");
+    if (!ctx->work) ctx->work = new Workspace();
+    Workspace& ws = *static_cast<Workspace*>(ctx->work);
+    cudaStream_t s = ctx->stream;
+    const size_t N = (size_t)net->N;
+    const int T = net->T, TS = net->term_states, n = net->n;
+    int st_ = ESL_OK;
+    SolveOut agg;
+
+    // ---- terminal kernels R_b (B x TS) ----
+    double* Rb = (double*)ws.get(S_RB, (size_t)B * TS * 8, &st_);
+    if (st_ != ESL_OK) return st_;
+    {
+        std::vector<int32_t> dense_list, big_list;
+        for (int t = 0; t < T; t++) {
+            int sz = net->h_offsets[t + 1] - net->h_offsets[t];
+            if (sz >= 2 && sz <= kDenseTerm) dense_list.push_back(t);
+            if (sz > kDenseTerm) big_list.push_back(t);
+        }
+        k_unit_terminals<<<dim3((T + 127) / 128, B), 128, 0, s>>>(T, net->offsets.get(), TS, Rb);
+        ESL_CUDA(cudaGetLastError());
+        if (!dense_list.empty()) {
+            int32_t* d_list = (int32_t*)ws.get(S_LIST, dense_list.size() * 4, &st_);
+            if (st_ != ESL_OK) return st_;
+            ESL_CUDA(cudaMemcpyAsync(d_list, dense_list.data(), dense_list.size() * 4, cudaMemcpyHostToDevice, s));
+            int smax = 0;
+            for (int t : dense_list) smax = std::max(smax, net->h_offsets[t + 1] - net->h_offsets[t]);
+            size_t smem = (size_t)smax * (smax + 1) * 8 + (size_t)smax * 4 + 16;
+            ESL_CUDA(cudaFuncSetAttribute(k_dense_terminal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_dense_terminal<<<dim3((unsigned)dense_list.size(), B), 256, smem, s>>>(
+                n, d_list, net->offsets.get(), net->order.get(), net->F.get(), d_rates, TS, Rb);
+            ESL_CUDA(cudaGetLastError());
+            ESL_CUDA(cudaStreamSynchronize(s));  // d_list is reused below
+        }
+        if (!big_list.empty()) {
+            // pin the first state of each big terminal SCC; solve the rest with Krylov
+            std::vector<uint8_t> h_big(T, 0);
+            for (int t : big_list) h_big[t] = 1;
+            uint8_t* d_big = (uint8_t*)ws.get(S_BIG, T, &st_);
+            uint8_t* d_pin = (uint8_t*)ws.get(S_PIN, N, &st_);
+            if (st_ != ESL_OK) return st_;
+            ESL_CUDA(cudaMemcpyAsync(d_big, h_big.data(), T, cudaMemcpyHostToDevice, s));
+            ESL_CUDA(cudaMemsetAsync(d_pin, 0, N, s));
+            std::vector<int32_t> pins;
+            std::vector<int32_t> h_order_first(big_list.size());
+            for (size_t j = 0; j < big_list.size(); j++)
+                ESL_CUDA(cudaMemcpyAsync(&h_order_first[j], net->order.get() + net->h_offsets[big_list[j]], 4,
+                                         cudaMemcpyDeviceToHost, s));
+            ESL_CUDA(cudaStreamSynchronize(s));
+            uint8_t one = 1;
+            for (int32_t v : h_order_first) ESL_CUDA(cudaMemcpyAsync(d_pin + v, &one, 1, cudaMemcpyHostToDevice, s));
+            ESL_CUDA(cudaStreamSynchronize(s));
+            Layout L;
+            ESL_TRY(make_layout(ctx, ws, net, 1, d_big, d_pin, true, L, 1, B));
+            const size_t vec = (size_t)B * L.ld;
+            double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
+            double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
+            double* sums = (double*)ws.get(S_SUM, (size_t)B * T * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            dim3 g = grid2(L.H, B);
+            k_rhs_pinned<<<g, kT, 0, s>>>(n, L.H, L.ld, d_rates, net->G.get(), d_pin, L.M0, L.M1, bE, bO);
+            ESL_CUDA(cudaGetLastError());
+            esl_solve_opts to = o;
+            to.tol = std::min(o.tol, 1e-12);
+            double *x64 = nullptr, *zE = nullptr;
+            SolveOut so;
+            ESL_TRY(krylov_solve<true>(ctx, ws, L, d_rates, B, bE, bO, nullptr, 0, to, x64, zE, so));
+            agg.iters += so.iters;
+            ESL_CUDA(cudaMemsetAsync(sums, 0, (size_t)B * T * 8, s));
+            dim3 gt((TS + kT - 1) / kT, B);
+            k_pinned_sum<<<gt, kT, 0, s>>>(T, net->offsets.get(), net->order.get(), d_big, d_pin, L.ld, zE, x64, TS,
+                                           Rb, sums);
+            k_pinned_norm<<<gt, kT, 0, s>>>(T, net->offsets.get(), d_big, TS, Rb, sums);
+            ESL_CUDA(cudaGetLastError());
+        }
+    }
+    if (d_R) ESL_CUDA(cudaMemcpyAsync(d_R, Rb, (size_t)TS * 8, cudaMemcpyDeviceToDevice, s));
+
+    // ---- transient part ----
+    const int K = B * R;
+    double* y = (double*)ws.get(S_Y, (size_t)K * T * 8, &st_);
+    if (st_ != ESL_OK) return st_;
+    ESL_CUDA(cudaMemsetAsync(y, 0, (size_t)K * T * 8, s));
+    const bool has_transient = (size_t)TS < N;
+    if (has_transient) {
+        Layout L;
+        ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, true, L, R, K));
+        const size_t vec = (size_t)K * L.ld;
+        double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
+        double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
+        if (st_ != ESL_OK) return st_;
+        dim3 g = grid2(L.H, K);
+        k_rhs<true><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
+        ESL_CUDA(cudaGetLastError());
+        double *x64 = nullptr, *zE = nullptr;
+        SolveOut so;
+        int rc = krylov_solve<true>(ctx, ws, L, d_rates, K, bE, bO, o.d_warm, N, o, x64, zE, so);
+        agg.iters += so.iters;
+        agg.refinements = so.refinements;
+        agg.relres = so.relres;
+        agg.converged = so.converged;
+        if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
+        k_terminal_mass<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, L.ld, d_rates, d_x0, N,
+                                                                    net->order.get(), net->term_of.get(),
+                                                                    net->G.get(), zE, x64, y);
+        ESL_CUDA(cudaGetLastError());
+        if (rc == ESL_ERR_NOT_CONVERGED) {
+            if (rep) {
+                rep->iterations = agg.iters;
+                rep->refinements = agg.refinements;
+                rep->relres = agg.relres;
+                rep->converged = 0;
+            }
+            return rc;
+        }
+    } else {
+        dim3 g((TS + 127) / 128, K);
+        k_terminal_mass<<<g, 128, 0, s>>>(n, T, TS, R, 0, d_rates, d_x0, N, net->order.get(), net->term_of.get(),
+                                          net->G.get(), nullptr, nullptr, y);
+        ESL_CUDA(cudaGetLastError());
+    }
+    // ---- x_inf and marginals ----
+    if (d_x_inf) {
+        ESL_CUDA(cudaMemsetAsync(d_x_inf, 0, (size_t)K * N * 8, s));
+        if (d_marg) ESL_CUDA(cudaMemsetAsync(d_marg, 0, (size_t)K * n * 8, s));
+        k_scatter_xinf<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, N, net->order.get(),
+                                                                   net->term_of.get(), Rb, y, d_x_inf, d_marg);
+        ESL_CUDA(cudaGetLastError());
+    }
+    // ---- absorption matrix L (backward form, first rate set) ----
+    if (d_L) {
+        if (has_transient) {
+            Layout L;
+            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, false, L, T, T));
+            const size_t vec = (size_t)T * L.ld;
+            double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
+            double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            dim3 g = grid2(L.H, T);
+            k_rhs<false><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
+            ESL_CUDA(cudaGetLastError());
+            double *x64 = nullptr, *zE = nullptr;
+            SolveOut so;
+            esl_solve_opts lo = o;
+            lo.d_warm = nullptr;
+            ESL_TRY(krylov_solve<false>(ctx, ws, L, d_rates, T, bE, bO, nullptr, 0, lo, x64, zE, so));
+            k_scatter_L<<<g, kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), zE, x64, d_L);
+            ESL_CUDA(cudaGetLastError());
+        } else {
+            // every state terminal: L[t][v] = [v in t]
+            ESL_CUDA(cudaMemsetAsync(d_L, 0, (size_t)T * N * 8, s));
+            Layout L;
+            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, false, L, T, T));
+            double* z = (double*)ws.get(S_BE, (size_t)T * L.ld * 8 * 2, &st_);
+            if (st_ != ESL_OK) return st_;
+            k_scatter_L<<<grid2(L.H, T), kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), z, z + (size_t)T * L.ld,
+                                                    d_L);
+            ESL_CUDA(cudaGetLastError());
+        }
+    }
+    ESL_CUDA(cudaStreamSynchronize(s));
+    if (rep) {
+        rep->iterations = agg.iters;
+        rep->refinements = agg.refinements;
+        rep->relres = agg.relres;
+        rep->converged = agg.converged ? 1 : 0;
+    }
+    return ESL_OK;
+}
+
+}  // namespace esl

@@ -1,0 +1,82 @@
+"""CPU-side checks of the C-ABI library: it loads, exports every declared symbol,
+and its host front end (bnet parsing, rate vectors) agrees with the oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import paraexastolog_b200 as esl
+from paraexastolog_b200 import synth
+
+
+def test_library_exports_every_declared_symbol():
+    L = esl.lib()
+    names = esl.header_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def _truth(off, pos, neg, i, states):
+    f = np.zeros(len(states), bool)
+    for c in range(off[i], off[i + 1]):
+        f |= ((states & pos[c]) == pos[c]) & ((states & neg[c]) == 0)
+    return f
+
+
+def _same_clauses(text):
+    """Same node list and the same truth function of every rule (the clause lists
+    may pick different never-true representatives for all-contradictory rules)."""
+    a = esl.Model.parse(text)
+    b = O.Model(text=text)
+    assert a.names == b.names
+    oa, pa, na = a.clauses()
+    ob, pb, nb = b.clauses()
+    states = np.arange(1 << a.n, dtype=np.int64) if a.n <= 16 else None
+    for i in range(a.n):
+        if states is not None:
+            assert np.array_equal(_truth(oa, pa, na, i, states), _truth(ob, pb, nb, i, states)), a.names[i]
+        else:
+            ca = sorted(zip(pa[oa[i]:oa[i + 1]].tolist(), na[oa[i]:oa[i + 1]].tolist()))
+            cb = sorted(zip(pb[ob[i]:ob[i + 1]].tolist(), nb[ob[i]:ob[i + 1]].tolist()))
+            assert ca == cb, (a.names[i], ca, cb)
+
+
+def test_parser_matches_oracle_on_reference_models(goldens):
+    for name, text in goldens["models"].items():
+        _same_clauses(text)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_parser_matches_oracle_on_generated(seed):
+    rng = np.random.default_rng(seed)
+    _same_clauses(synth.random_table_network(rng, 8, [1, 2, 3, 4], 0.5).bnet)
+    _same_clauses(synth.nested_canalizing_network(rng, 9, 3).bnet)
+
+
+def test_parser_quirks():
+    assert esl.Model.parse("targets, factors\nA, A\nB, !A").names == ["A"]
+    assert esl.Model.parse("A, A\nB, !A\n").names == ["A", "B"]
+    _same_clauses("targets, factors\nA, A\nB, A & X\n")
+    _same_clauses("targets, factors\nA, (A & X & !X) | B\nB, B\n")
+    _same_clauses("targets, factors\nA, !(A | !(B & (A | !B)))\nB, !!B\n")
+    _same_clauses("targets,\tfactors\nA,\tA & !A\nB, B\n")
+    with pytest.raises(esl.EslError):
+        esl.Model.parse("targets, factors\nA, (A & \nB, B\n")
+    with pytest.raises(esl.EslError):
+        esl.Model.parse("targets, factors\nA, (X & !X) | (Y & !Y)\nB, B\n")
+
+
+def test_rates_host_api(goldens):
+    m = esl.Model.parse(goldens["models"]["toy.bnet"])
+    r = m.rates_uniform(down={"C": 2.0})
+    assert r.tolist() == [1, 1, 1, 2, 1, 1]
+    with pytest.raises(esl.EslError):
+        m.rates_uniform(up={"Z": 1.0})
+    with pytest.raises(esl.EslError):
+        m.rates_uniform(up={"A": -1.0})
+    a = m.rates_normal(1.0, 0.5)
+    b = m.rates_normal(1.0, 0.5)
+    assert np.array_equal(a, b) and np.all(a >= 0)
+    assert m.rates_normal(1.0, 0.5, up={"A": 7.0})[0] == 7.0
