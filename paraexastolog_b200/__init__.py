@@ -105,6 +105,8 @@ def _ptr(t) -> Optional[int]:
         return None
     if isinstance(t, np.ndarray):
         return t.ctypes.data
+    if t.numel() == 0:  # an empty view still points at its (non-empty) buffer
+        return t.untyped_storage().data_ptr()
     return t.data_ptr()
 
 

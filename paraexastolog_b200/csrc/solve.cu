@@ -30,7 +30,9 @@
 // refinement loop: the true residual is always formed in FP64, the inner solve runs
 // in FP64 (ESL_METHOD_FP64) or FP32 (ESL_METHOD_MIXED).  All operators are applied
 // matrix-free from the flip masks and the rates.
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "esl_internal.h"
@@ -51,9 +53,14 @@ __device__ __forceinline__ uint32_t nb_half(uint32_t h, int i) { return i == 0 ?
 struct KState {
     double rho, alpha, omega, beta;
     double r0v, ts, tt, r0r, rr;
-    double rnorm2_true, bnorm2, target2;
-    int done, iters, breakdown, pad;
+    double rnorm2_true, bnorm2, target2, prev_r2, rnorm2_trial;
+    int done, iters, breakdown, pad, noimp, pad2;
 };
+
+// A system whose true FP64 residual stops improving (a refinement step no longer
+// halves it) has reached the accuracy FP64 can deliver for it; it is accepted when
+// that residual is within kAcceptRel of ||b||.
+constexpr double kAcceptRel = 1e-8;
 
 template <class T>
 __device__ __forceinline__ void load_rates(T* s_rate, const double* __restrict__ rates, int b, int n) {
@@ -117,7 +124,16 @@ struct Layout {
     const uint32_t* M1; // odd-half coupling masks | domain bit
     const uint32_t* F0; // even-half out-masks
     const uint32_t* F1; // odd-half out-masks
+    // pinned terminal systems: state pins[k*T + terminal] is fixed to 1 in system k
+    const int32_t* pins;
+    const int32_t* term_of;
+    int T;
 };
+
+// pinned state of the row's SCC in system k, or -1
+__device__ __forceinline__ int32_t row_pin(const Layout& L, int k, uint32_t v) {
+    return L.pins ? L.pins[(size_t)k * L.T + L.term_of[v]] : -1;
+}
 
 // wE[h] = (bE[h] + sum_i c_i x1[nb]) / q  on the even half (bE may be null)
 template <bool FWD, class T, class TX>
@@ -138,12 +154,18 @@ __global__ void __launch_bounds__(kT) k_elim(Layout L, const double* __restrict_
         return;
     }
     uint32_t v = state_of(h, 0);
+    const int32_t pin = row_pin(L, k, v);
+    if ((int32_t)v == pin) {
+        wE[o + h] = 0;
+        return;
+    }
     T acc = bE ? (T)bE[o + h] : (T)0;
     if (x1) {
         uint32_t mm = m & kMaskBits;
         while (mm) {
             int i = __ffs(mm) - 1;
             mm &= mm - 1;
+            if ((int32_t)(v ^ (1u << i)) == pin) continue;
             acc += coupling<FWD>(s_rate, i, v) * (T)x1[o + nb_half(h, i)];
         }
     }
@@ -153,6 +175,7 @@ __global__ void __launch_bounds__(kT) k_elim(Layout L, const double* __restrict_
 // Odd-half operator.  mode 0: y = S x (and dot r0.y -> st.r0v);
 // mode 2: y = S x with x = s / dS, dots (y . dS x) -> ts and (y . y) -> tt;
 // mode 3: residual r = b - S x (FP64) with r.r -> rnorm2_true;
+// mode 5: as mode 3 for a trial iterate, r.r -> rnorm2_trial (systems with an inner solve);
 // mode 4: rhs  y = b + sum_i c_i w[nb]  (x unused).
 template <bool FWD, int MODE, class T, class TX>
 __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict__ rates, const TX* __restrict__ x,
@@ -161,7 +184,8 @@ __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict
                                               T* __restrict__ y, KState* __restrict__ st) {
     __shared__ T s_rate[64];
     const int k = blockIdx.y;
-    if (st && MODE != 3 && MODE != 4 && st[k].done) return;
+    if (st && MODE != 3 && MODE != 4 && MODE != 5 && st[k].done) return;
+    if (MODE == 5 && st[k].pad) return;
     load_rates(s_rate, rates, k / L.nrhs, L.n);
     __syncthreads();
     uint32_t h = blockIdx.x * kT + threadIdx.x;
@@ -169,16 +193,18 @@ __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict
     double d0 = 0, d1 = 0;
     if (h < L.H) {
         uint32_t m = L.M1[h];
+        const uint32_t v = state_of(h, 1);
+        const int32_t pin = (m & kDomainBit) ? row_pin(L, k, v) : -1;
         T out;
-        if (!(m & kDomainBit)) {
-            out = MODE == 4 ? (T)0 : (MODE == 3 ? (T)0 : (T)x[o + h]);
+        if (!(m & kDomainBit) || (int32_t)v == pin) {
+            out = MODE == 4 ? (T)0 : ((MODE == 3 || MODE == 5) ? (T)0 : (T)x[o + h]);
         } else {
-            uint32_t v = state_of(h, 1);
             T acc = 0;
             uint32_t mm = m & kMaskBits;
             while (mm) {
                 int i = __ffs(mm) - 1;
                 mm &= mm - 1;
+                if ((int32_t)(v ^ (1u << i)) == pin) continue;
                 acc += coupling<FWD>(s_rate, i, v) * wE[o + nb_half(h, i)];
             }
             if (MODE == 4) {
@@ -186,7 +212,7 @@ __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict
             } else {
                 T q = out_rate(s_rate, L.F1[h], v);
                 T sx = q * (T)x[o + h] - acc;
-                out = MODE == 3 ? (T)b[o + h] - sx : sx;
+                out = (MODE == 3 || MODE == 5) ? (T)b[o + h] - sx : sx;
             }
         }
         y[o + h] = out;
@@ -195,11 +221,12 @@ __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict
             d0 = (double)out * (double)x[o + h] * dS[o + h];
             d1 = (double)out * (double)out;
         }
-        if (MODE == 3) d0 = (double)out * (double)out;
+        if (MODE == 3 || MODE == 5) d0 = (double)out * (double)out;
     }
     if (MODE == 0) block_sum2(d0, 0.0, &st[k].r0v, nullptr);
     if (MODE == 2) block_sum2(d0, d1, &st[k].ts, &st[k].tt);
     if (MODE == 3) block_sum2(d0, 0.0, &st[k].rnorm2_true, nullptr);
+    if (MODE == 5) block_sum2(d0, 0.0, &st[k].rnorm2_trial, nullptr);
 }
 
 // Schur diagonal dS[h] = q_o - sum_i c_i(o) c_i(e)/q_e over odd states o (1 outside the domain)
@@ -213,16 +240,18 @@ __global__ void __launch_bounds__(kT) k_schur_diag(Layout L, const double* __res
     if (h >= L.H) return;
     const size_t o = (size_t)k * L.ld;
     uint32_t m = L.M1[h];
-    if (!(m & kDomainBit)) {
+    const uint32_t v = state_of(h, 1);
+    const int32_t pin = (m & kDomainBit) ? row_pin(L, k, v) : -1;
+    if (!(m & kDomainBit) || (int32_t)v == pin) {
         dS[o + h] = 1.0;
         return;
     }
-    uint32_t v = state_of(h, 1);
     double d = out_rate(s_rate, L.F1[h], v);
     uint32_t mm = m & kMaskBits;
     while (mm) {
         int i = __ffs(mm) - 1;
         mm &= mm - 1;
+        if ((int32_t)(v ^ (1u << i)) == pin) continue;
         uint32_t he = nb_half(h, i);
         uint32_t me = L.M0[he];
         if ((me >> i) & 1u) {
@@ -339,13 +368,16 @@ __global__ void k_scal_beta(int K, KState* st, int max_iters) {
 }
 
 // after the true residual: decide which systems still need an inner solve
-__global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2, int* n_active) {
+__global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2, int outer, int* n_active) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     KState& s = st[k];
     bool conv = s.rnorm2_true <= tol2 * s.bnorm2 || s.bnorm2 == 0.0;
-    s.done = conv ? 1 : 0;
-    if (!conv) {
+    bool stalled = outer > 0 && (s.noimp || s.rnorm2_true > 0.25 * s.prev_r2) &&
+                   s.rnorm2_true <= kAcceptRel * kAcceptRel * s.bnorm2;
+    s.prev_r2 = s.rnorm2_true;
+    s.done = (conv || stalled) ? 1 : 0;
+    if (!s.done) {
         atomicAdd(n_active, 1);
         s.rho = s.rnorm2_true;  // r0 = r at the start: rho = r0.r
         s.alpha = s.omega = 1.0;
@@ -359,15 +391,47 @@ __global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2,
 }
 
 
+// xt = x + d for systems that ran an inner solve
 template <class T>
-__global__ void k_add_correction(Layout L, double* __restrict__ x64, const T* __restrict__ d,
-                                 const KState* __restrict__ st) {
+__global__ void k_trial(Layout L, const double* __restrict__ x64, const T* __restrict__ d, double* __restrict__ xt,
+                        const KState* __restrict__ st) {
     const int k = blockIdx.y;
-    if (st[k].pad) return;  // pad marks systems that had no inner solve this round
+    if (st[k].pad) return;
     uint32_t h = blockIdx.x * kT + threadIdx.x;
     if (h >= L.H) return;
     size_t i = (size_t)k * L.ld + h;
-    x64[i] += (double)d[i];
+    xt[i] = x64[i] + (double)d[i];
+}
+
+// keep the trial iterate only where it lowered the true residual
+__global__ void k_commit_flags(int K, KState* st, int* n_noimp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    KState& s = st[k];
+    s.noimp = 0;
+    if (s.pad) return;
+    if (s.rnorm2_trial < s.rnorm2_true) {
+        s.rnorm2_true = s.rnorm2_trial;
+    } else {
+        s.noimp = 1;
+        atomicAdd(n_noimp, 1);
+    }
+}
+
+__global__ void k_commit(Layout L, double* __restrict__ x64, double* __restrict__ r64, const double* __restrict__ xt,
+                         const double* __restrict__ rt, const KState* __restrict__ st) {
+    const int k = blockIdx.y;
+    if (st[k].pad || st[k].noimp) return;
+    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    if (h >= L.H) return;
+    size_t i = (size_t)k * L.ld + h;
+    x64[i] = xt[i];
+    r64[i] = rt[i];
+}
+
+__global__ void k_zero_trial(int K, KState* st) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) st[k].rnorm2_trial = 0.0;
 }
 
 __global__ void k_mark_inner(int K, KState* st) {
@@ -571,66 +635,93 @@ __global__ void k_unit_terminals(int T, const int32_t* __restrict__ offsets, int
 }
 
 // half-layout masks for one domain; domain(v) decided by `dom`:
-// dom = 0: transient states; dom = 1: states of "big" terminal SCCs except their pinned state
+// dom = 0: transient states; dom = 1: states of "big" terminal SCCs
 __global__ void k_half_masks(int n, uint32_t H, const uint32_t* __restrict__ Md, const uint32_t* __restrict__ F,
-                             const int32_t* __restrict__ term_of, const uint8_t* __restrict__ big_term,
-                             const uint8_t* __restrict__ is_pin, int dom, uint32_t* __restrict__ M0,
-                             uint32_t* __restrict__ M1, uint32_t* __restrict__ F0, uint32_t* __restrict__ F1) {
+                             const int32_t* __restrict__ term_of, const uint8_t* __restrict__ big_term, int dom,
+                             uint32_t* __restrict__ M0, uint32_t* __restrict__ M1, uint32_t* __restrict__ F0,
+                             uint32_t* __restrict__ F1) {
     uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= H) return;
     for (int par = 0; par < 2; par++) {
         uint32_t v = state_of(h, par);
         int t = term_of[v];
-        bool in;
-        if (dom == 0) in = t < 0;
-        else in = t >= 0 && big_term[t] && !is_pin[v];
-        uint32_t m = Md[v];
-        if (dom == 1 && in) {
-            // neighbours that are the pinned state are not unknowns
-            uint32_t mm = m, keep = 0;
-            while (mm) {
-                int i = __ffs(mm) - 1;
-                mm &= mm - 1;
-                if (!is_pin[v ^ (1u << i)]) keep |= 1u << i;
-            }
-            m = keep;
-        }
-        (par ? M1 : M0)[h] = in ? (m | kDomainBit) : 0u;
+        bool in = dom == 0 ? t < 0 : (t >= 0 && big_term[t]);
+        (par ? M1 : M0)[h] = in ? (Md[v] | kDomainBit) : 0u;
         (par ? F1 : F0)[h] = F[v];
     }
 }
 
+// Pin of each (big terminal SCC, rate set): the state with the largest ratio of
+// in-rate to out-rate, a cheap proxy for the largest stationary mass; pinning a
+// high-mass state keeps the remaining system well conditioned.  Ties -> smallest state.
+__global__ void k_pin_score(int n, int T, int term_states, const int32_t* __restrict__ order,
+                            const int32_t* __restrict__ term_of, const uint8_t* __restrict__ big_term,
+                            const uint32_t* __restrict__ F, const uint32_t* __restrict__ G,
+                            const double* __restrict__ rates, unsigned long long* __restrict__ best) {
+    const int b = blockIdx.y;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= term_states) return;
+    uint32_t v = (uint32_t)order[p];
+    int t = term_of[v];
+    if (!big_term[t]) return;
+    const double* rt = rates + (size_t)b * 2 * n;
+    double in = 0.0, out = 0.0;
+    uint32_t g = G[v], f = F[v];
+    while (g) {
+        int i = __ffs(g) - 1;
+        g &= g - 1;
+        uint32_t u = v ^ (1u << i);
+        in += rt[2 * i + ((u >> i) & 1u)];
+    }
+    while (f) {
+        int i = __ffs(f) - 1;
+        f &= f - 1;
+        out += rt[2 * i + ((v >> i) & 1u)];
+    }
+    float score = (float)(in / out);  // positive: its bits order like unsigned ints
+    unsigned long long key = ((unsigned long long)__float_as_uint(score) << 32) | (0xFFFFFFFFull - v);
+    atomicMax(&best[(size_t)b * T + t], key);
+}
+
+__global__ void k_pin_decode(int count, const unsigned long long* __restrict__ best, int32_t* __restrict__ pins) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    unsigned long long key = best[j];
+    pins[j] = key ? (int32_t)(0xFFFFFFFFull - (key & 0xFFFFFFFFull)) : -1;
+}
+
 // pinned terminal systems: rhs b_v = rate(pin -> v) for states v of a big terminal SCC
-__global__ void k_rhs_pinned(int n, uint32_t H, size_t ld, const double* __restrict__ rates,
-                             const uint32_t* __restrict__ G, const uint8_t* __restrict__ is_pin,
-                             const uint32_t* __restrict__ M0, const uint32_t* __restrict__ M1,
+__global__ void k_rhs_pinned(Layout L, const double* __restrict__ rates, const uint32_t* __restrict__ G,
                              double* __restrict__ bE, double* __restrict__ bO) {
     __shared__ double s_rate[64];
     const int k = blockIdx.y;
-    load_rates(s_rate, rates, k, n);
+    load_rates(s_rate, rates, k, L.n);
     __syncthreads();
     uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= H) return;
+    if (h >= L.H) return;
     for (int par = 0; par < 2; par++) {
         uint32_t v = state_of(h, par);
-        uint32_t m = (par ? M1 : M0)[h];
+        uint32_t m = (par ? L.M1 : L.M0)[h];
         double val = 0.0;
         if (m & kDomainBit) {
-            uint32_t g = G[v];
-            while (g) {
-                int i = __ffs(g) - 1;
-                g &= g - 1;
-                uint32_t u = v ^ (1u << i);
-                if (is_pin[u]) val += s_rate[2 * i + ((u >> i) & 1u)];
+            const int32_t pin = row_pin(L, k, v);
+            if ((int32_t)v != pin) {
+                uint32_t g = G[v];
+                while (g) {
+                    int i = __ffs(g) - 1;
+                    g &= g - 1;
+                    uint32_t u = v ^ (1u << i);
+                    if ((int32_t)u == pin) val += s_rate[2 * i + ((u >> i) & 1u)];
+                }
             }
         }
-        (par ? bO : bE)[(size_t)k * ld + h] = val;
+        (par ? bO : bE)[(size_t)k * L.ld + h] = val;
     }
 }
 
 // R for big terminal SCCs from the pinned solution z (pin = 1), normalised per SCC
 __global__ void k_pinned_sum(int T, const int32_t* __restrict__ offsets, const int32_t* __restrict__ order,
-                             const uint8_t* __restrict__ big_term, const uint8_t* __restrict__ is_pin, size_t ld,
+                             const uint8_t* __restrict__ big_term, const int32_t* __restrict__ pins, size_t ld,
                              const double* __restrict__ zE, const double* __restrict__ zO, int term_states,
                              double* __restrict__ Rb, double* __restrict__ sums) {
     const int b = blockIdx.y;
@@ -647,7 +738,7 @@ __global__ void k_pinned_sum(int T, const int32_t* __restrict__ offsets, const i
         t = lo;
     }
     if (!big_term[t]) return;
-    double val = is_pin[v] ? 1.0 : fabs((__popc(v) & 1) ? zO[(size_t)b * ld + (v >> 1)] : zE[(size_t)b * ld + (v >> 1)]);
+    double val = (int32_t)v == pins[(size_t)b * T + t] ? 1.0 : fabs((__popc(v) & 1) ? zO[(size_t)b * ld + (v >> 1)] : zE[(size_t)b * ld + (v >> 1)]);
     Rb[(size_t)b * term_states + p] = val;
     atomicAdd(&sums[(size_t)b * T + t], val);
 }
@@ -704,6 +795,12 @@ __global__ void k_half_from_full(uint32_t H, size_t ld, const double* __restrict
     uint32_t h = blockIdx.x * kT + threadIdx.x;
     if (h >= H) return;
     x1[(size_t)k * ld + h] = (M1[h] & kDomainBit) ? full[(size_t)k * full_ld + state_of(h, 1)] : 0.0;
+}
+
+bool debug_enabled() {
+    static int on = -1;
+    if (on < 0) on = getenv("ESL_DEBUG") ? 1 : 0;
+    return on == 1;
 }
 
 template <class T>
@@ -781,7 +878,7 @@ namespace {
 enum Slot {
     S_BE, S_BS, S_DS, S_X64, S_R64, S_W64, S_ZE, S_ST, S_ACT,
     S_R, S_R0, S_PH, S_V, S_SH, S_T, S_D, S_W,
-    S_M0, S_M1, S_F0, S_F1, S_RB, S_Y, S_SUM, S_BIG, S_PIN, S_BO, S_LIST, S_COUNT
+    S_M0, S_M1, S_F0, S_F1, S_RB, S_Y, S_SUM, S_BIG, S_PIN, S_BO, S_LIST, S_XT, S_RT, S_COUNT
 };
 
 struct SolveOut {
@@ -805,7 +902,7 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     double* w64 = (double*)ws.get(S_W64, vec * 8, &st_);
     double* zE = (double*)ws.get(S_ZE, vec * 8, &st_);
     KState* st = (KState*)ws.get(S_ST, (size_t)K * sizeof(KState), &st_);
-    int* n_active = (int*)ws.get(S_ACT, sizeof(int), &st_);
+    int* n_active = (int*)ws.get(S_ACT, 2 * sizeof(int), &st_);
     const bool mixed = o.method == ESL_METHOD_MIXED;
     const size_t tsz = mixed ? 4 : 8;
     void* iv_p[8];
@@ -829,33 +926,59 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     const double floor_rel = mixed ? 3e-6 : 1e-13;
     int total_iters = 0, outer = 0;
     int active = 0;
+    bool inner64 = !mixed;
+    double* xt = (double*)ws.get(S_XT, vec * 8, &st_);
+    double* rt = (double*)ws.get(S_RT, vec * 8, &st_);
+    if (st_ != ESL_OK) return st_;
+    // true residual of the starting iterate
+    k_zero_r<<<sb, 128, 0, s>>>(K, st);
+    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
+    k_apply<FWD, 3, double, double><<<g, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
     for (;; outer++) {
-        k_zero_r<<<sb, 128, 0, s>>>(K, st);
-        k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
-        k_apply<FWD, 3, double, double><<<g, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
-        ESL_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s));
+        ESL_CUDA(cudaMemsetAsync(n_active, 0, 2 * sizeof(int), s));
         // inner target: a relative reduction that reaches tol in one inner solve,
         // but not below what the inner precision can deliver
-        k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_rel * floor_rel, n_active);
+        const double floor_now = inner64 ? 1e-13 : floor_rel;
+        k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_now * floor_now, outer, n_active);
         ESL_CUDA(cudaGetLastError());
         ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
         ESL_CUDA(cudaStreamSynchronize(s));
+        if (debug_enabled()) {
+            std::vector<KState> h_st(K);
+            ESL_CUDA(cudaMemcpy(h_st.data(), st, (size_t)K * sizeof(KState), cudaMemcpyDeviceToHost));
+            for (int k = 0; k < K && k < 4; k++)
+                fprintf(stderr, "[esl] outer %d sys %d relres %.3e inner64 %d breakdown %d\n", outer, k,
+                        h_st[k].bnorm2 > 0 ? std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2) : 0.0, (int)inner64,
+                        h_st[k].breakdown);
+        }
         if (active == 0 || outer >= o.max_refine) break;
         k_mark_inner<<<sb, 128, 0, s>>>(K, st);
         int it = 0;
-        if (mixed) {
+        k_zero_trial<<<sb, 128, 0, s>>>(K, st);
+        if (!inner64) {
             InnerVecs<float> iv{(float*)iv_p[0], (float*)iv_p[1], (float*)iv_p[2], (float*)iv_p[3],
                                 (float*)iv_p[4], (float*)iv_p[5], (float*)iv_p[6], (float*)iv_p[7]};
             ESL_TRY((inner_bicgstab<FWD, float>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
-            k_add_correction<float><<<g, kT, 0, s>>>(L, x64, iv.d, st);
+            k_trial<float><<<g, kT, 0, s>>>(L, x64, iv.d, xt, st);
         } else {
             InnerVecs<double> iv{(double*)iv_p[0], (double*)iv_p[1], (double*)iv_p[2], (double*)iv_p[3],
                                  (double*)iv_p[4], (double*)iv_p[5], (double*)iv_p[6], (double*)iv_p[7]};
             ESL_TRY((inner_bicgstab<FWD, double>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
-            k_add_correction<double><<<g, kT, 0, s>>>(L, x64, iv.d, st);
+            k_trial<double><<<g, kT, 0, s>>>(L, x64, iv.d, xt, st);
         }
-        ESL_CUDA(cudaGetLastError());
         total_iters += it;
+        // true residual of the trial iterate; commit where it improved
+        k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, xt, nullptr, w64, nullptr);
+        k_apply<FWD, 5, double, double><<<g, kT, 0, s>>>(L, rates, xt, w64, dS, bS, nullptr, rt, st);
+        ESL_CUDA(cudaMemsetAsync(n_active + 1, 0, sizeof(int), s));
+        k_commit_flags<<<sb, 128, 0, s>>>(K, st, n_active + 1);
+        k_commit<<<g, kT, 0, s>>>(L, x64, r64, xt, rt, st);
+        ESL_CUDA(cudaGetLastError());
+        int noimp = 0;
+        ESL_CUDA(cudaMemcpyAsync(&noimp, n_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        // an FP32 correction that did not help: continue in FP64
+        if (noimp > 0 && !inner64) inner64 = true;
     }
     // even half: zE = (bE + A_eo x) / q_e
     k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, bE, zE, nullptr);
@@ -869,27 +992,30 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     out.iters = total_iters;
     out.refinements = outer;
     out.relres = worst;
-    out.converged = active == 0;
+    out.converged = active == 0 || worst <= kAcceptRel;
     x64_out = x64;
     zE_out = zE;
     if (!out.converged)
-        return fail(ESL_ERR_NOT_CONVERGED, "relative residual " + std::to_string(worst) + " above tolerance after " +
-                                               std::to_string(outer) + " refinement steps");
+    {
+        char msg[160];
+        snprintf(msg, sizeof msg, "relative residual %.3e above tolerance after %d refinement steps", worst, outer);
+        return fail(ESL_ERR_NOT_CONVERGED, msg);
+    }
     return ESL_OK;
 }
 
-int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const uint8_t* big_term,
-                const uint8_t* is_pin, bool fwd, Layout& L, int nrhs, int K) {
+int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const uint8_t* big_term, bool fwd,
+                Layout& L, int nrhs) {
     int st_ = ESL_OK;
     const uint32_t H = (uint32_t)(net->N / 2);
-    uint32_t* M0 = (uint32_t*)ws.get(S_M0 + 0, (size_t)H * 4 * 4, &st_);
+    uint32_t* M0 = (uint32_t*)ws.get(S_M0, (size_t)H * 4 * 4, &st_);
     if (st_ != ESL_OK) return st_;
     uint32_t* M1 = M0 + H;
     uint32_t* F0 = M0 + 2 * (size_t)H;
     uint32_t* F1 = M0 + 3 * (size_t)H;
     k_half_masks<<<(H + kT - 1) / kT, kT, 0, ctx->stream>>>(net->n, H, fwd ? net->Gdom.get() : net->Fdom.get(),
-                                                           net->F.get(), net->term_of.get(), big_term, is_pin, dom, M0,
-                                                           M1, F0, F1);
+                                                           net->F.get(), net->term_of.get(), big_term, dom, M0, M1,
+                                                           F0, F1);
     ESL_CUDA(cudaGetLastError());
     L.n = net->n;
     L.H = H;
@@ -899,7 +1025,9 @@ int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const 
     L.M1 = M1;
     L.F0 = F0;
     L.F1 = F1;
-    (void)K;
+    L.pins = nullptr;
+    L.term_of = nullptr;
+    L.T = 0;
     return ESL_OK;
 }
 
@@ -957,45 +1085,50 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_CUDA(cudaStreamSynchronize(s));  // d_list is reused below
         }
         if (!big_list.empty()) {
-            // pin the first state of each big terminal SCC; solve the rest with Krylov
+            // pin one high-mass state per (big terminal SCC, rate set); solve the rest with Krylov
             std::vector<uint8_t> h_big(T, 0);
             for (int t : big_list) h_big[t] = 1;
             uint8_t* d_big = (uint8_t*)ws.get(S_BIG, T, &st_);
-            uint8_t* d_pin = (uint8_t*)ws.get(S_PIN, N, &st_);
+            unsigned long long* d_best = (unsigned long long*)ws.get(S_PIN, (size_t)B * T * 8, &st_);
+            int32_t* d_pins = (int32_t*)ws.get(S_LIST, (size_t)B * T * 4, &st_);
             if (st_ != ESL_OK) return st_;
             ESL_CUDA(cudaMemcpyAsync(d_big, h_big.data(), T, cudaMemcpyHostToDevice, s));
-            ESL_CUDA(cudaMemsetAsync(d_pin, 0, N, s));
-            std::vector<int32_t> pins;
-            std::vector<int32_t> h_order_first(big_list.size());
-            for (size_t j = 0; j < big_list.size(); j++)
-                ESL_CUDA(cudaMemcpyAsync(&h_order_first[j], net->order.get() + net->h_offsets[big_list[j]], 4,
-                                         cudaMemcpyDeviceToHost, s));
-            ESL_CUDA(cudaStreamSynchronize(s));
-            uint8_t one = 1;
-            for (int32_t v : h_order_first) ESL_CUDA(cudaMemcpyAsync(d_pin + v, &one, 1, cudaMemcpyHostToDevice, s));
-            ESL_CUDA(cudaStreamSynchronize(s));
+            ESL_CUDA(cudaMemsetAsync(d_best, 0, (size_t)B * T * 8, s));
+            dim3 gt((TS + kT - 1) / kT, B);
+            k_pin_score<<<gt, kT, 0, s>>>(n, T, TS, net->order.get(), net->term_of.get(), d_big, net->F.get(),
+                                          net->G.get(), d_rates, d_best);
+            k_pin_decode<<<(unsigned)((B * T + 255) / 256), 256, 0, s>>>(B * T, d_best, d_pins);
+            ESL_CUDA(cudaGetLastError());
             Layout L;
-            ESL_TRY(make_layout(ctx, ws, net, 1, d_big, d_pin, true, L, 1, B));
+            ESL_TRY(make_layout(ctx, ws, net, 1, d_big, true, L, 1));
+            L.pins = d_pins;
+            L.term_of = net->term_of.get();
+            L.T = T;
             const size_t vec = (size_t)B * L.ld;
             double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
             double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
             double* sums = (double*)ws.get(S_SUM, (size_t)B * T * 8, &st_);
             if (st_ != ESL_OK) return st_;
             dim3 g = grid2(L.H, B);
-            k_rhs_pinned<<<g, kT, 0, s>>>(n, L.H, L.ld, d_rates, net->G.get(), d_pin, L.M0, L.M1, bE, bO);
+            k_rhs_pinned<<<g, kT, 0, s>>>(L, d_rates, net->G.get(), bE, bO);
             ESL_CUDA(cudaGetLastError());
+            // terminal kernels are solved in FP64 throughout: they can be badly
+            // conditioned and their cost is small next to the transient part
             esl_solve_opts to = o;
+            to.method = ESL_METHOD_FP64;
             to.tol = std::min(o.tol, 1e-12);
+            to.d_warm = nullptr;
+            to.max_refine = std::max(o.max_refine, 8);
             double *x64 = nullptr, *zE = nullptr;
             SolveOut so;
             ESL_TRY(krylov_solve<true>(ctx, ws, L, d_rates, B, bE, bO, nullptr, 0, to, x64, zE, so));
             agg.iters += so.iters;
             ESL_CUDA(cudaMemsetAsync(sums, 0, (size_t)B * T * 8, s));
-            dim3 gt((TS + kT - 1) / kT, B);
-            k_pinned_sum<<<gt, kT, 0, s>>>(T, net->offsets.get(), net->order.get(), d_big, d_pin, L.ld, zE, x64, TS,
+            k_pinned_sum<<<gt, kT, 0, s>>>(T, net->offsets.get(), net->order.get(), d_big, d_pins, L.ld, zE, x64, TS,
                                            Rb, sums);
             k_pinned_norm<<<gt, kT, 0, s>>>(T, net->offsets.get(), d_big, TS, Rb, sums);
             ESL_CUDA(cudaGetLastError());
+            ESL_CUDA(cudaStreamSynchronize(s));
         }
     }
     if (d_R) ESL_CUDA(cudaMemcpyAsync(d_R, Rb, (size_t)TS * 8, cudaMemcpyDeviceToDevice, s));
@@ -1008,7 +1141,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     const bool has_transient = (size_t)TS < N;
     if (has_transient) {
         Layout L;
-        ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, true, L, R, K));
+        ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, true, L, R));
         const size_t vec = (size_t)K * L.ld;
         double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
         double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
@@ -1055,7 +1188,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     if (d_L) {
         if (has_transient) {
             Layout L;
-            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, false, L, T, T));
+            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, false, L, T));
             const size_t vec = (size_t)T * L.ld;
             double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
             double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
@@ -1074,7 +1207,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             // every state terminal: L[t][v] = [v in t]
             ESL_CUDA(cudaMemsetAsync(d_L, 0, (size_t)T * N * 8, s));
             Layout L;
-            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, nullptr, false, L, T, T));
+            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, false, L, T));
             double* z = (double*)ws.get(S_BE, (size_t)T * L.ld * 8 * 2, &st_);
             if (st_ != ESL_OK) return st_;
             k_scatter_L<<<grid2(L.H, T), kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), z, z + (size_t)T * L.ld,
