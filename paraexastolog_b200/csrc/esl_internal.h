@@ -101,6 +101,12 @@ struct esl_net {
     esl::DevBuf<uint32_t> Gdom;       // in-mask restricted to same-class neighbours
     esl::DevBuf<uint32_t> Fdom;       // out-mask restricted to same-class neighbours
     int max_terminal = 0;             // largest terminal SCC
+    // level-group plan of the block forward solve, built on first use
+    void* plan = nullptr;
+    void (*plan_free)(void*) = nullptr;
+    ~esl_net() {
+        if (plan && plan_free) plan_free(plan);
+    }
 };
 
 namespace esl {

@@ -30,6 +30,7 @@
 // refinement loop: the true residual is always formed in FP64, the inner solve runs
 // in FP64 (ESL_METHOD_FP64) or FP32 (ESL_METHOD_MIXED).  All operators are applied
 // matrix-free from the flip masks and the rates.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -54,13 +55,18 @@ struct KState {
     double rho, alpha, omega, beta;
     double r0v, ts, tt, r0r, rr;
     double rnorm2_true, bnorm2, target2, prev_r2, rnorm2_trial;
-    int done, iters, breakdown, pad, noimp, pad2;
+    int done, iters, breakdown, pad, noimp, total_iters;
 };
 
 // A system whose true FP64 residual stops improving (a refinement step no longer
 // halves it) has reached the accuracy FP64 can deliver for it; it is accepted when
 // that residual is within kAcceptRel of ||b||.
 constexpr double kAcceptRel = 1e-8;
+// iteration budget of each level-group solve of the block forward solve; systems
+// that miss it have the group's SCC blocks (up to kDenseFallbackMax states) solved
+// by dense LU instead
+constexpr int kBlockBudget = 3000;
+constexpr int kDenseFallbackMax = 4096;
 
 template <class T>
 __device__ __forceinline__ void load_rates(T* s_rate, const double* __restrict__ rates, int b, int n) {
@@ -128,7 +134,28 @@ struct Layout {
     const int32_t* pins;
     const int32_t* term_of;
     int T;
+    // when set, blockIdx.y indexes this list of running systems
+    const int32_t* act;
+    // when set, rows are restricted to these half indices (even / odd parity)
+    const uint32_t* list0;
+    const uint32_t* list1;
+    uint32_t n0, n1;
 };
+
+__device__ __forceinline__ int sys_index(const Layout& L) { return L.act ? L.act[blockIdx.y] : (int)blockIdx.y; }
+
+// half index of this thread's row of the given parity; false past the last row
+__device__ __forceinline__ bool row_h(const Layout& L, int parity, uint32_t& h) {
+    const uint32_t idx = blockIdx.x * kT + threadIdx.x;
+    const uint32_t* list = parity ? L.list1 : L.list0;
+    if (list) {
+        if (idx >= (parity ? L.n1 : L.n0)) return false;
+        h = list[idx];
+        return true;
+    }
+    h = idx;
+    return idx < L.H;
+}
 
 // pinned state of the row's SCC in system k, or -1
 __device__ __forceinline__ int32_t row_pin(const Layout& L, int k, uint32_t v) {
@@ -141,12 +168,12 @@ __global__ void __launch_bounds__(kT) k_elim(Layout L, const double* __restrict_
                                              const double* __restrict__ bE, T* __restrict__ wE,
                                              const KState* __restrict__ st) {
     __shared__ T s_rate[64];
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st && st[k].done) return;
     load_rates(s_rate, rates, k / L.nrhs, L.n);
     __syncthreads();
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 0, h)) return;
     const size_t o = (size_t)k * L.ld;
     uint32_t m = L.M0[h];
     if (!(m & kDomainBit)) {
@@ -183,15 +210,16 @@ __global__ void __launch_bounds__(kT) k_apply(Layout L, const double* __restrict
                                               const double* __restrict__ b, const T* __restrict__ r0,
                                               T* __restrict__ y, KState* __restrict__ st) {
     __shared__ T s_rate[64];
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st && MODE != 3 && MODE != 4 && MODE != 5 && st[k].done) return;
     if (MODE == 5 && st[k].pad) return;
     load_rates(s_rate, rates, k / L.nrhs, L.n);
     __syncthreads();
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    uint32_t h = 0;
+    const bool valid = row_h(L, 1, h);
     const size_t o = (size_t)k * L.ld;
     double d0 = 0, d1 = 0;
-    if (h < L.H) {
+    if (valid) {
         uint32_t m = L.M1[h];
         const uint32_t v = state_of(h, 1);
         const int32_t pin = (m & kDomainBit) ? row_pin(L, k, v) : -1;
@@ -236,8 +264,8 @@ __global__ void __launch_bounds__(kT) k_schur_diag(Layout L, const double* __res
     const int k = blockIdx.y;
     load_rates(s_rate, rates, k / L.nrhs, L.n);
     __syncthreads();
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     const size_t o = (size_t)k * L.ld;
     uint32_t m = L.M1[h];
     const uint32_t v = state_of(h, 1);
@@ -267,10 +295,10 @@ __global__ void __launch_bounds__(kT) k_schur_diag(Layout L, const double* __res
 template <class T>
 __global__ void k_inner_start(Layout L, const double* __restrict__ r64, T* __restrict__ r, T* __restrict__ r0,
                               T* __restrict__ d, T* __restrict__ ph, T* __restrict__ v, const KState* __restrict__ st) {
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st[k].done) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     size_t i = (size_t)k * L.ld + h;
     T val = (T)r64[i];
     r[i] = val;
@@ -283,10 +311,10 @@ __global__ void k_inner_start(Layout L, const double* __restrict__ r64, T* __res
 template <class T>
 __global__ void k_update_p(Layout L, const double* __restrict__ dS, const T* __restrict__ r, T* __restrict__ ph,
                            const T* __restrict__ v, const KState* __restrict__ st) {
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st[k].done) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     size_t i = (size_t)k * L.ld + h;
     T beta = (T)st[k].beta, omega = (T)st[k].omega;
     T inv = (T)(1.0 / dS[i]);
@@ -296,10 +324,10 @@ __global__ void k_update_p(Layout L, const double* __restrict__ dS, const T* __r
 template <class T>
 __global__ void k_update_s(Layout L, const double* __restrict__ dS, const T* __restrict__ r, const T* __restrict__ v,
                            T* __restrict__ sh, const KState* __restrict__ st) {
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st[k].done) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     size_t i = (size_t)k * L.ld + h;
     T alpha = (T)st[k].alpha;
     sh[i] = (r[i] - alpha * v[i]) * (T)(1.0 / dS[i]);
@@ -310,11 +338,12 @@ __global__ void __launch_bounds__(kT) k_update_xr(Layout L, const double* __rest
                                                   T* __restrict__ r, const T* __restrict__ r0,
                                                   const T* __restrict__ ph, const T* __restrict__ sh,
                                                   const T* __restrict__ t, KState* __restrict__ st) {
-    const int k = blockIdx.y;
+    const int k = sys_index(L);
     if (st[k].done) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    uint32_t h = 0;
+    const bool valid = row_h(L, 1, h);
     double a = 0, b = 0;
-    if (h < L.H) {
+    if (valid) {
         size_t i = (size_t)k * L.ld + h;
         T alpha = (T)st[k].alpha, omega = (T)st[k].omega;
         d[i] += alpha * ph[i] + omega * sh[i];
@@ -353,7 +382,15 @@ __global__ void k_scal_beta(int K, KState* st, int max_iters) {
     if (k >= K || st[k].done) return;
     KState& s = st[k];
     s.iters++;
+    s.total_iters++;
     if (s.rr <= s.target2 || s.iters >= max_iters) {
+        s.done = 1;
+        return;
+    }
+    // BiCGStab residuals grow transiently (by 1e5 in squared norm on these systems);
+    // only a blow-up beyond 1e20 or a NaN stops the inner solve
+    if (!(s.rr <= 1e20 * s.rnorm2_true)) {
+        s.breakdown = 2;
         s.done = 1;
         return;
     }
@@ -368,7 +405,8 @@ __global__ void k_scal_beta(int K, KState* st, int max_iters) {
 }
 
 // after the true residual: decide which systems still need an inner solve
-__global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2, int outer, int* n_active) {
+__global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2, int outer, int budget,
+                              int* n_active) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     KState& s = st[k];
@@ -376,7 +414,7 @@ __global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2,
     bool stalled = outer > 0 && (s.noimp || s.rnorm2_true > 0.25 * s.prev_r2) &&
                    s.rnorm2_true <= kAcceptRel * kAcceptRel * s.bnorm2;
     s.prev_r2 = s.rnorm2_true;
-    s.done = (conv || stalled) ? 1 : 0;
+    s.done = (conv || stalled || s.total_iters >= budget) ? 1 : 0;
     if (!s.done) {
         atomicAdd(n_active, 1);
         s.rho = s.rnorm2_true;  // r0 = r at the start: rho = r0.r
@@ -397,8 +435,8 @@ __global__ void k_trial(Layout L, const double* __restrict__ x64, const T* __res
                         const KState* __restrict__ st) {
     const int k = blockIdx.y;
     if (st[k].pad) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     size_t i = (size_t)k * L.ld + h;
     xt[i] = x64[i] + (double)d[i];
 }
@@ -422,8 +460,8 @@ __global__ void k_commit(Layout L, double* __restrict__ x64, double* __restrict_
                          const double* __restrict__ rt, const KState* __restrict__ st) {
     const int k = blockIdx.y;
     if (st[k].pad || st[k].noimp) return;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= L.H) return;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
     size_t i = (size_t)k * L.ld + h;
     x64[i] = xt[i];
     r64[i] = rt[i];
@@ -773,28 +811,37 @@ __global__ void k_scatter_L(uint32_t H, int T, size_t N, size_t ld, const int32_
 }
 
 // ---- driver ---------------------------------------------------------------------------------
-__global__ void k_count_running(int K, const KState* st, int* n) {
+
+// list of running systems (order irrelevant)
+__global__ void k_active_list(int K, const KState* st, int* n, int32_t* list) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < K && !st[k].done) atomicAdd(n, 1);
+    if (k < K && !st[k].done) list[atomicAdd(n, 1)] = k;
 }
 
-__global__ void __launch_bounds__(kT) k_norm2(uint32_t H, size_t ld, const double* __restrict__ x, KState* st) {
+__global__ void __launch_bounds__(kT) k_norm2(Layout L, const double* __restrict__ x, KState* st) {
     const int k = blockIdx.y;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
+    uint32_t h = 0;
+    const bool valid = row_h(L, 1, h);
     double a = 0.0;
-    if (h < H) {
-        double v = x[(size_t)k * ld + h];
+    if (valid) {
+        double v = x[(size_t)k * L.ld + h];
         a = v * v;
     }
     block_sum2(a, 0.0, &st[k].bnorm2, nullptr);
 }
 
-__global__ void k_half_from_full(uint32_t H, size_t ld, const double* __restrict__ full, size_t full_ld,
-                                 const uint32_t* __restrict__ M1, double* __restrict__ x1) {
+__global__ void k_half_from_full(Layout L, const double* __restrict__ full, size_t full_ld, double* __restrict__ x1) {
     const int k = blockIdx.y;
-    uint32_t h = blockIdx.x * kT + threadIdx.x;
-    if (h >= H) return;
-    x1[(size_t)k * ld + h] = (M1[h] & kDomainBit) ? full[(size_t)k * full_ld + state_of(h, 1)] : 0.0;
+    uint32_t h;
+    if (!row_h(L, 1, h)) return;
+    x1[(size_t)k * L.ld + h] = (L.M1[h] & kDomainBit) ? full[(size_t)k * full_ld + state_of(h, 1)] : 0.0;
+}
+
+__global__ void k_zero_rows(Layout L, int parity, double* __restrict__ x) {
+    const int k = blockIdx.y;
+    uint32_t h;
+    if (!row_h(L, parity, h)) return;
+    x[(size_t)k * L.ld + h] = 0.0;
 }
 
 bool debug_enabled() {
@@ -809,36 +856,43 @@ struct InnerVecs {
 };
 
 inline dim3 grid2(uint32_t H, int K) { return dim3((H + kT - 1) / kT, (unsigned)K); }
+inline dim3 grid_rows(const Layout& L, int parity, int K) {
+    uint32_t rows = (parity ? L.list1 : L.list0) ? (parity ? L.n1 : L.n0) : L.H;
+    return dim3((std::max(rows, 1u) + kT - 1) / kT, (unsigned)K);
+}
 
 template <bool FWD, class T>
-int inner_bicgstab(esl_ctx* ctx, const Layout& L, const double* rates, int K, const double* dS, const double* r64,
-                   KState* st, int* n_active, InnerVecs<T> iv, int max_iters, int* iters_out) {
+int inner_bicgstab(esl_ctx* ctx, Layout L, const double* rates, int K, const double* dS, const double* r64,
+                   KState* st, int* n_active, int32_t* act, InnerVecs<T> iv, int max_iters, int* iters_out) {
     cudaStream_t s = ctx->stream;
-    dim3 g = grid2(L.H, K);
     unsigned sb = (unsigned)((K + 127) / 128);
-    k_inner_start<T><<<g, kT, 0, s>>>(L, r64, iv.r, iv.r0, iv.d, iv.ph, iv.v, st);
+    L.act = nullptr;
+    k_inner_start<T><<<grid_rows(L, 1, K), kT, 0, s>>>(L, r64, iv.r, iv.r0, iv.d, iv.ph, iv.v, st);
     int it = 0;
     const int check_every = 8;
     while (it < max_iters) {
-        for (int c = 0; c < check_every; c++, it++) {
-            k_update_p<T><<<g, kT, 0, s>>>(L, dS, iv.r, iv.ph, iv.v, st);
-            k_elim<FWD, T, T><<<g, kT, 0, s>>>(L, rates, iv.ph, nullptr, iv.w, st);
-            k_apply<FWD, 0, T, T><<<g, kT, 0, s>>>(L, rates, iv.ph, iv.w, dS, nullptr, iv.r0, iv.v, st);
-            k_scal_alpha<<<sb, 128, 0, s>>>(K, st);
-            k_update_s<T><<<g, kT, 0, s>>>(L, dS, iv.r, iv.v, iv.sh, st);
-            k_elim<FWD, T, T><<<g, kT, 0, s>>>(L, rates, iv.sh, nullptr, iv.w, st);
-            k_apply<FWD, 2, T, T><<<g, kT, 0, s>>>(L, rates, iv.sh, iv.w, dS, nullptr, nullptr, iv.t, st);
-            k_scal_omega<<<sb, 128, 0, s>>>(K, st);
-            k_update_xr<T><<<g, kT, 0, s>>>(L, dS, iv.d, iv.r, iv.r0, iv.ph, iv.sh, iv.t, st);
-            k_scal_beta<<<sb, 128, 0, s>>>(K, st, max_iters);
-        }
-        ESL_CUDA(cudaGetLastError());
+        // launch only over the systems still running
         ESL_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s));
-        k_count_running<<<sb, 128, 0, s>>>(K, st, n_active);
+        k_active_list<<<sb, 128, 0, s>>>(K, st, n_active, act);
         int active = 0;
         ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
         ESL_CUDA(cudaStreamSynchronize(s));
         if (active == 0) break;
+        L.act = act;
+        const dim3 g0 = grid_rows(L, 0, active), g1 = grid_rows(L, 1, active);
+        for (int c = 0; c < check_every; c++, it++) {
+            k_update_p<T><<<g1, kT, 0, s>>>(L, dS, iv.r, iv.ph, iv.v, st);
+            k_elim<FWD, T, T><<<g0, kT, 0, s>>>(L, rates, iv.ph, nullptr, iv.w, st);
+            k_apply<FWD, 0, T, T><<<g1, kT, 0, s>>>(L, rates, iv.ph, iv.w, dS, nullptr, iv.r0, iv.v, st);
+            k_scal_alpha<<<sb, 128, 0, s>>>(K, st);
+            k_update_s<T><<<g1, kT, 0, s>>>(L, dS, iv.r, iv.v, iv.sh, st);
+            k_elim<FWD, T, T><<<g0, kT, 0, s>>>(L, rates, iv.sh, nullptr, iv.w, st);
+            k_apply<FWD, 2, T, T><<<g1, kT, 0, s>>>(L, rates, iv.sh, iv.w, dS, nullptr, nullptr, iv.t, st);
+            k_scal_omega<<<sb, 128, 0, s>>>(K, st);
+            k_update_xr<T><<<g1, kT, 0, s>>>(L, dS, iv.d, iv.r, iv.r0, iv.ph, iv.sh, iv.t, st);
+            k_scal_beta<<<sb, 128, 0, s>>>(K, st, max_iters);
+        }
+        ESL_CUDA(cudaGetLastError());
     }
     *iters_out = it;
     return ESL_OK;
@@ -865,6 +919,11 @@ struct Workspace {
         }
         return b.first;
     }
+    void swap(int a, int b) {
+        int m = std::max(a, b);
+        if ((int)bufs.size() <= m) bufs.resize(m + 1, {nullptr, 0});
+        std::swap(bufs[a], bufs[b]);
+    }
     ~Workspace() {
         for (auto& b : bufs)
             if (b.first) cudaFree(b.first);
@@ -878,13 +937,14 @@ namespace {
 enum Slot {
     S_BE, S_BS, S_DS, S_X64, S_R64, S_W64, S_ZE, S_ST, S_ACT,
     S_R, S_R0, S_PH, S_V, S_SH, S_T, S_D, S_W,
-    S_M0, S_M1, S_F0, S_F1, S_RB, S_Y, S_SUM, S_BIG, S_PIN, S_BO, S_LIST, S_XT, S_RT, S_COUNT
+    S_M0, S_M1, S_F0, S_F1, S_RB, S_Y, S_SUM, S_BIG, S_PIN, S_BO, S_LIST, S_XT, S_RT, S_ACTLIST, S_ZEF, S_ZOF, S_ZEB, S_ZOB, S_RSUB, S_XSUB, S_LUOFF, S_LUSYS, S_LU, S_COUNT
 };
 
 struct SolveOut {
     int iters = 0, refinements = 0;
     double relres = 0.0;
     bool converged = true;
+    std::vector<double> sys_relres;  // per system, from the last Krylov solve
 };
 
 // Solves the K systems whose rhs halves are in (bE, bO); solution in x64 (odd) and zE (even).
@@ -903,27 +963,31 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     double* zE = (double*)ws.get(S_ZE, vec * 8, &st_);
     KState* st = (KState*)ws.get(S_ST, (size_t)K * sizeof(KState), &st_);
     int* n_active = (int*)ws.get(S_ACT, 2 * sizeof(int), &st_);
+    int32_t* act = (int32_t*)ws.get(S_ACTLIST, (size_t)K * sizeof(int32_t), &st_);
     const bool mixed = o.method == ESL_METHOD_MIXED;
-    const size_t tsz = mixed ? 4 : 8;
+    // sized for FP64 elements even in mixed mode: a mixed solve may continue with
+    // FP64 inner iterations on the same buffers
     void* iv_p[8];
-    for (int j = 0; j < 8; j++) iv_p[j] = ws.get(S_R + j, vec * tsz, &st_);
+    for (int j = 0; j < 8; j++) iv_p[j] = ws.get(S_R + j, vec * sizeof(double), &st_);
     if (st_ != ESL_OK) return st_;
-    dim3 g = grid2(L.H, K);
+    const dim3 g0 = grid_rows(L, 0, K), g1 = grid_rows(L, 1, K);
     unsigned sb = (unsigned)((K + 127) / 128);
     ESL_CUDA(cudaMemsetAsync(st, 0, (size_t)K * sizeof(KState), s));
-    k_schur_diag<FWD><<<g, kT, 0, s>>>(L, rates, dS);
+    k_schur_diag<FWD><<<g1, kT, 0, s>>>(L, rates, dS);
     // reduced rhs: bS = bO + A_oe (bE / q_e)
-    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, (const double*)nullptr, bE, w64, nullptr);
-    k_apply<FWD, 4, double, double><<<g, kT, 0, s>>>(L, rates, (const double*)nullptr, w64, dS, bO, nullptr, bS,
-                                                     nullptr);
-    k_norm2<<<g, kT, 0, s>>>(L.H, L.ld, bS, st);
+    k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, (const double*)nullptr, bE, w64, nullptr);
+    k_apply<FWD, 4, double, double><<<g1, kT, 0, s>>>(L, rates, (const double*)nullptr, w64, dS, bO, nullptr, bS,
+                                                      nullptr);
+    k_norm2<<<g1, kT, 0, s>>>(L, bS, st);
     if (warm)
-        k_half_from_full<<<g, kT, 0, s>>>(L.H, L.ld, warm, warm_ld, L.M1, x64);
+        k_half_from_full<<<g1, kT, 0, s>>>(L, warm, warm_ld, x64);
     else
-        ESL_CUDA(cudaMemsetAsync(x64, 0, vec * 8, s));
+        k_zero_rows<<<g1, kT, 0, s>>>(L, 1, x64);
     ESL_CUDA(cudaGetLastError());
     const double tol = o.tol > 0 ? o.tol : 1e-10;
-    const double floor_rel = mixed ? 3e-6 : 1e-13;
+    // FP32 inner solves stop at 1e-4 relative: below that the FP32 operator's
+    // rounding (cancellation between the diagonal and the neighbour flow) dominates
+    const double floor_rel = mixed ? 1e-4 : 1e-13;
     int total_iters = 0, outer = 0;
     int active = 0;
     bool inner64 = !mixed;
@@ -932,24 +996,28 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     if (st_ != ESL_OK) return st_;
     // true residual of the starting iterate
     k_zero_r<<<sb, 128, 0, s>>>(K, st);
-    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
-    k_apply<FWD, 3, double, double><<<g, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
+    k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
+    k_apply<FWD, 3, double, double><<<g1, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
     for (;; outer++) {
         ESL_CUDA(cudaMemsetAsync(n_active, 0, 2 * sizeof(int), s));
         // inner target: a relative reduction that reaches tol in one inner solve,
         // but not below what the inner precision can deliver
         const double floor_now = inner64 ? 1e-13 : floor_rel;
-        k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_now * floor_now, outer, n_active);
+        k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_now * floor_now, outer, o.max_iters, n_active);
         ESL_CUDA(cudaGetLastError());
         ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
         ESL_CUDA(cudaStreamSynchronize(s));
         if (debug_enabled()) {
             std::vector<KState> h_st(K);
             ESL_CUDA(cudaMemcpy(h_st.data(), st, (size_t)K * sizeof(KState), cudaMemcpyDeviceToHost));
-            for (int k = 0; k < K && k < 4; k++)
-                fprintf(stderr, "[esl] outer %d sys %d relres %.3e inner64 %d breakdown %d\n", outer, k,
-                        h_st[k].bnorm2 > 0 ? std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2) : 0.0, (int)inner64,
-                        h_st[k].breakdown);
+            int shown = 0;
+            for (int k = 0; k < K && shown < 6; k++) {
+                double rel = h_st[k].bnorm2 > 0 ? std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2) : 0.0;
+                if (k >= 2 && rel <= tol) continue;
+                shown++;
+                fprintf(stderr, "[esl] outer %d sys %d/%d relres %.3e b2 %.3e inner64 %d breakdown %d iters %d\n", outer,
+                        k, K, rel, h_st[k].bnorm2, (int)inner64, h_st[k].breakdown, h_st[k].iters);
+            }
         }
         if (active == 0 || outer >= o.max_refine) break;
         k_mark_inner<<<sb, 128, 0, s>>>(K, st);
@@ -958,21 +1026,21 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
         if (!inner64) {
             InnerVecs<float> iv{(float*)iv_p[0], (float*)iv_p[1], (float*)iv_p[2], (float*)iv_p[3],
                                 (float*)iv_p[4], (float*)iv_p[5], (float*)iv_p[6], (float*)iv_p[7]};
-            ESL_TRY((inner_bicgstab<FWD, float>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
-            k_trial<float><<<g, kT, 0, s>>>(L, x64, iv.d, xt, st);
+            ESL_TRY((inner_bicgstab<FWD, float>(ctx, L, rates, K, dS, r64, st, n_active, act, iv, o.max_iters, &it)));
+            k_trial<float><<<g1, kT, 0, s>>>(L, x64, iv.d, xt, st);
         } else {
             InnerVecs<double> iv{(double*)iv_p[0], (double*)iv_p[1], (double*)iv_p[2], (double*)iv_p[3],
                                  (double*)iv_p[4], (double*)iv_p[5], (double*)iv_p[6], (double*)iv_p[7]};
-            ESL_TRY((inner_bicgstab<FWD, double>(ctx, L, rates, K, dS, r64, st, n_active, iv, o.max_iters, &it)));
-            k_trial<double><<<g, kT, 0, s>>>(L, x64, iv.d, xt, st);
+            ESL_TRY((inner_bicgstab<FWD, double>(ctx, L, rates, K, dS, r64, st, n_active, act, iv, o.max_iters, &it)));
+            k_trial<double><<<g1, kT, 0, s>>>(L, x64, iv.d, xt, st);
         }
         total_iters += it;
         // true residual of the trial iterate; commit where it improved
-        k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, xt, nullptr, w64, nullptr);
-        k_apply<FWD, 5, double, double><<<g, kT, 0, s>>>(L, rates, xt, w64, dS, bS, nullptr, rt, st);
+        k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, xt, nullptr, w64, nullptr);
+        k_apply<FWD, 5, double, double><<<g1, kT, 0, s>>>(L, rates, xt, w64, dS, bS, nullptr, rt, st);
         ESL_CUDA(cudaMemsetAsync(n_active + 1, 0, sizeof(int), s));
         k_commit_flags<<<sb, 128, 0, s>>>(K, st, n_active + 1);
-        k_commit<<<g, kT, 0, s>>>(L, x64, r64, xt, rt, st);
+        k_commit<<<g1, kT, 0, s>>>(L, x64, r64, xt, rt, st);
         ESL_CUDA(cudaGetLastError());
         int noimp = 0;
         ESL_CUDA(cudaMemcpyAsync(&noimp, n_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -981,24 +1049,429 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
         if (noimp > 0 && !inner64) inner64 = true;
     }
     // even half: zE = (bE + A_eo x) / q_e
-    k_elim<FWD, double, double><<<g, kT, 0, s>>>(L, rates, x64, bE, zE, nullptr);
+    k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, x64, bE, zE, nullptr);
     ESL_CUDA(cudaGetLastError());
     std::vector<KState> h_st(K);
     ESL_CUDA(cudaMemcpyAsync(h_st.data(), st, (size_t)K * sizeof(KState), cudaMemcpyDeviceToHost, s));
     ESL_CUDA(cudaStreamSynchronize(s));
     double worst = 0.0;
-    for (auto& k : h_st)
-        if (k.bnorm2 > 0) worst = std::max(worst, std::sqrt(k.rnorm2_true / k.bnorm2));
+    out.sys_relres.assign(K, 0.0);
+    for (int k = 0; k < K; k++)
+        if (h_st[k].bnorm2 > 0) {
+            out.sys_relres[k] = std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2);
+            worst = std::max(worst, out.sys_relres[k]);
+        }
+    if (debug_enabled()) {
+        std::vector<int> its;
+        long long sum = 0;
+        for (auto& k : h_st) {
+            its.push_back(k.total_iters);
+            sum += k.total_iters;
+        }
+        std::sort(its.begin(), its.end());
+        fprintf(stderr, "[esl] K=%d inner iterations per system: mean %.1f min %d p50 %d p90 %d p99 %d max %d\n", K,
+                (double)sum / K, its.front(), its[K / 2], its[(K * 9) / 10], its[(K * 99) / 100], its.back());
+        for (int k = 0; k < K; k++)
+            if (h_st[k].total_iters > 1000)
+                fprintf(stderr, "[esl]   hard system %d iterations %d relres %.3e\n", k, h_st[k].total_iters,
+                        h_st[k].bnorm2 > 0 ? std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2) : 0.0);
+    }
     out.iters = total_iters;
     out.refinements = outer;
     out.relres = worst;
-    out.converged = active == 0 || worst <= kAcceptRel;
+    // residual-based: a system that ran out of budget is done but not converged
+    out.converged = worst <= kAcceptRel;
     x64_out = x64;
     zE_out = zE;
     if (!out.converged)
     {
         char msg[160];
         snprintf(msg, sizeof msg, "relative residual %.3e above tolerance after %d refinement steps", worst, outer);
+        return fail(ESL_ERR_NOT_CONVERGED, msg);
+    }
+    return ESL_OK;
+}
+
+
+// ---- block forward solve over SCC levels --------------------------------------------------
+// The transient part is block lower-triangular in topological order: the SCCs of
+// one level depend only on SCCs of higher levels (sources come first), never on
+// each other.  Levels are solved in order; a level of singleton SCCs is a direct
+// division, any other level a Krylov solve restricted to its states (block-diagonal
+// over its SCCs).  This is the reference's block-triangular structure
+// (cuda/src/linear_system_solve.cu:249-325) with the per-block LU replaced by
+// direct/Krylov solves, and it is exact in the inter-block coupling.
+struct BlockPlan {
+    std::vector<uint32_t> off0, off1;  // group offsets into list0 / list1
+    std::vector<int> max_scc;          // largest SCC of each group
+    DevBuf<uint32_t> list0, list1;     // half indices of each group's even / odd states
+    DevBuf<uint32_t> hm;               // half-layout masks: M0, M1 (same-SCC in-edges | domain), F0, F1
+    DevBuf<uint32_t> Gx;               // per state: in-edges from other transient SCCs
+    // SCCs of each group up to kDenseFallbackMax states (first position in `order`, size), for the LU fallback
+    std::vector<uint32_t> off_scc;
+    std::vector<int64_t> lu_doubles;   // dense scratch of one system for each group
+    DevBuf<int32_t> scc_beg, scc_size;
+};
+
+void free_plan(void* p) { delete static_cast<BlockPlan*>(p); }
+
+__global__ void k_scc_masks(int n, uint64_t N, const uint32_t* __restrict__ F, const uint32_t* __restrict__ G,
+                            const int32_t* __restrict__ lab, const int32_t* __restrict__ term_of,
+                            uint32_t* __restrict__ Gx, uint32_t* __restrict__ hm, uint32_t H) {
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const bool transient = term_of[v] < 0;
+    uint32_t g = G[v], same = 0, cross = 0;
+    const int32_t c = lab[v];
+    while (g) {
+        int i = __ffs(g) - 1;
+        g &= g - 1;
+        uint64_t u = v ^ (1ull << i);
+        if (term_of[u] >= 0) continue;
+        if (lab[u] == c) same |= 1u << i;
+        else cross |= 1u << i;
+    }
+    Gx[v] = transient ? cross : 0u;
+    const uint32_t h = (uint32_t)(v >> 1);
+    const int par = __popcll(v) & 1;
+    hm[(size_t)par * H + h] = transient ? (same | kDomainBit) : 0u;
+    hm[(size_t)(2 + par) * H + h] = F[v];
+}
+
+// Dense LU fallback for transient SCC blocks (forward form), one CTA per (SCC, system):
+// rows = equations of the SCC's states, A[a][a] = out-rate, A[a][b] = -rate(b -> a) for
+// edges inside the SCC, rhs = the group rhs already formed in bE / bO.  Gaussian
+// elimination with partial pivoting in a global scratch matrix (s x (s+1), row-major).
+__global__ void __launch_bounds__(256) k_dense_block(int n, const int32_t* __restrict__ scc_beg,
+                                                     const int32_t* __restrict__ scc_size,
+                                                     const int64_t* __restrict__ scc_scratch,
+                                                     const int32_t* __restrict__ sys, int64_t sys_stride,
+                                                     const int32_t* __restrict__ order,
+                                                     const uint32_t* __restrict__ F, const uint32_t* __restrict__ G,
+                                                     const double* __restrict__ rates, int nrhs, size_t ld,
+                                                     const double* __restrict__ bE, const double* __restrict__ bO,
+                                                     double* __restrict__ ZE, double* __restrict__ ZO,
+                                                     double* __restrict__ scratch) {
+    __shared__ double s_rate[64];
+    __shared__ int s_piv;
+    __shared__ double s_red[32];
+    __shared__ int s_redi[32];
+    const int j = blockIdx.x;
+    const int k = sys[blockIdx.y];
+    const int beg = scc_beg[j], sz = scc_size[j];
+    const int ldA = sz + 1;
+    double* A = scratch + (size_t)blockIdx.y * sys_stride + scc_scratch[j];
+    const int32_t* mem = order + beg;
+    load_rates(s_rate, rates, k / nrhs, n);
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)sz * ldA; e += blockDim.x) A[e] = 0.0;
+    __syncthreads();
+    for (int a = threadIdx.x; a < sz; a += blockDim.x) {
+        const uint32_t v = (uint32_t)mem[a];
+        A[(size_t)a * ldA + a] = out_rate(s_rate, F[v], v);
+        uint32_t g = G[v];
+        while (g) {
+            int i = __ffs(g) - 1;
+            g &= g - 1;
+            const int32_t u = (int32_t)(v ^ (1u << i));
+            int lo = 0, hi = sz - 1;  // members ascending
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (mem[mid] < u) lo = mid + 1; else hi = mid;
+            }
+            if (mem[lo] == u) A[(size_t)a * ldA + lo] -= s_rate[2 * i + (((uint32_t)u >> i) & 1u)];
+        }
+        const size_t o = (size_t)k * ld + (v >> 1);
+        A[(size_t)a * ldA + sz] = (__popc(v) & 1) ? bO[o] : bE[o];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int col = 0; col < sz; col++) {
+        double best = -1.0;
+        int bi = col;
+        for (int r = col + threadIdx.x; r < sz; r += blockDim.x) {
+            double a = fabs(A[(size_t)r * ldA + col]);
+            if (a > best) { best = a; bi = r; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+            int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (lane == 0) { s_red[warp] = best; s_redi[warp] = bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b0 = s_red[0];
+            int i0 = s_redi[0];
+            for (int w = 1; w < nw; w++)
+                if (s_red[w] > b0 || (s_red[w] == b0 && s_redi[w] < i0)) { b0 = s_red[w]; i0 = s_redi[w]; }
+            s_piv = i0;
+        }
+        __syncthreads();
+        const int piv = s_piv;
+        if (piv != col)
+            for (int c = col + threadIdx.x; c <= sz; c += blockDim.x) {
+                double t = A[(size_t)col * ldA + c];
+                A[(size_t)col * ldA + c] = A[(size_t)piv * ldA + c];
+                A[(size_t)piv * ldA + c] = t;
+            }
+        __syncthreads();
+        const double inv = 1.0 / A[(size_t)col * ldA + col];
+        const int rows = sz - col - 1, cols = sz - col;
+        for (int64_t e = threadIdx.x; e < (int64_t)rows * cols; e += blockDim.x) {
+            const int r = col + 1 + (int)(e / cols), c = col + 1 + (int)(e % cols);
+            A[(size_t)r * ldA + c] -= A[(size_t)r * ldA + col] * inv * A[(size_t)col * ldA + c];
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        for (int r = sz - 1; r >= 0; r--) {
+            double acc = 0.0;
+            for (int c = r + 1 + lane; c < sz; c += 32) acc += A[(size_t)r * ldA + c] * A[(size_t)c * ldA + sz];
+            acc = warp_sum(acc);
+            if (lane == 0) A[(size_t)r * ldA + sz] = (A[(size_t)r * ldA + sz] - acc) / A[(size_t)r * ldA + r];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int a = threadIdx.x; a < sz; a += blockDim.x) {
+        const uint32_t v = (uint32_t)mem[a];
+        const size_t o = (size_t)k * ld + (v >> 1);
+        ((__popc(v) & 1) ? ZO : ZE)[o] = A[(size_t)a * ldA + sz];
+    }
+}
+
+int get_plan(esl_ctx* ctx, const esl_net* net, BlockPlan*& out) {
+    if (net->plan) {
+        out = static_cast<BlockPlan*>(net->plan);
+        return ESL_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    const size_t N = (size_t)net->N;
+    const uint32_t H = (uint32_t)(N / 2);
+    auto* P = new BlockPlan();
+    std::vector<int32_t> order(N), offsets(net->n_sccs + 1), levels(net->n_sccs);
+    int rc = ESL_OK;
+    auto chk = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == ESL_OK) rc = fail(ESL_ERR_CUDA, cudaGetErrorString(e));
+    };
+    chk(cudaMemcpyAsync(order.data(), net->order.get(), N * 4, cudaMemcpyDeviceToHost, s));
+    chk(cudaMemcpyAsync(offsets.data(), net->offsets.get(), offsets.size() * 4, cudaMemcpyDeviceToHost, s));
+    chk(cudaMemcpyAsync(levels.data(), net->levels.get(), levels.size() * 4, cudaMemcpyDeviceToHost, s));
+    chk(cudaStreamSynchronize(s));
+    if (rc != ESL_OK) {
+        delete P;
+        return rc;
+    }
+    std::vector<uint32_t> l0, l1;
+    std::vector<int32_t> sb, ss;
+    P->off0.push_back(0);
+    P->off1.push_back(0);
+    P->off_scc.push_back(0);
+    for (int c = net->T; c < net->n_sccs;) {
+        int c1 = c, mx = 0;
+        int64_t lu = 0;
+        while (c1 < net->n_sccs && levels[c1] == levels[c]) {
+            const int sz = offsets[c1 + 1] - offsets[c1];
+            mx = std::max(mx, sz);
+            if (sz <= kDenseFallbackMax) {  // singletons too: a failed Krylov iterate is redone everywhere
+                sb.push_back(offsets[c1]);
+                ss.push_back(sz);
+                lu += (int64_t)sz * (sz + 1);
+            }
+            for (int p = offsets[c1]; p < offsets[c1 + 1]; p++) {
+                uint32_t v = (uint32_t)order[p];
+                (__builtin_popcount(v) & 1 ? l1 : l0).push_back(v >> 1);
+            }
+            c1++;
+        }
+        P->off0.push_back((uint32_t)l0.size());
+        P->off1.push_back((uint32_t)l1.size());
+        P->off_scc.push_back((uint32_t)sb.size());
+        P->lu_doubles.push_back(lu);
+        P->max_scc.push_back(mx);
+        c = c1;
+    }
+    rc = P->list0.alloc(l0.size());
+    if (rc == ESL_OK) rc = P->scc_beg.alloc(sb.size());
+    if (rc == ESL_OK) rc = P->scc_size.alloc(ss.size());
+    if (rc == ESL_OK && !sb.empty()) {
+        chk(cudaMemcpyAsync(P->scc_beg.get(), sb.data(), sb.size() * 4, cudaMemcpyHostToDevice, s));
+        chk(cudaMemcpyAsync(P->scc_size.get(), ss.data(), ss.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    if (rc == ESL_OK) rc = P->list1.alloc(l1.size());
+    if (rc == ESL_OK) rc = P->hm.alloc((size_t)4 * H);
+    if (rc == ESL_OK) rc = P->Gx.alloc(N);
+    if (rc == ESL_OK) {
+        if (!l0.empty()) chk(cudaMemcpyAsync(P->list0.get(), l0.data(), l0.size() * 4, cudaMemcpyHostToDevice, s));
+        if (!l1.empty()) chk(cudaMemcpyAsync(P->list1.get(), l1.data(), l1.size() * 4, cudaMemcpyHostToDevice, s));
+        k_scc_masks<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(net->n, N, net->F.get(), net->G.get(),
+                                                                net->labels.get(), net->term_of.get(), P->Gx.get(),
+                                                                P->hm.get(), H);
+        chk(cudaGetLastError());
+        chk(cudaStreamSynchronize(s));
+    }
+    if (rc != ESL_OK) {
+        delete P;
+        return rc;
+    }
+    esl_net* mnet = const_cast<esl_net*>(net);
+    mnet->plan = P;
+    mnet->plan_free = free_plan;
+    out = P;
+    return ESL_OK;
+}
+
+// rhs of one level group: b_v = x0(v) + inflow from already solved transient states;
+// `direct` groups (singleton SCCs only) store z_v = b_v / q_v immediately.
+__global__ void __launch_bounds__(kT) k_group_rhs(Layout L, int parity, const double* __restrict__ rates,
+                                                  const double* __restrict__ x0, size_t x0_ld,
+                                                  const uint32_t* __restrict__ Gx, const double* __restrict__ ZE,
+                                                  const double* __restrict__ ZO, double* __restrict__ b, int direct,
+                                                  double* __restrict__ Zout) {
+    __shared__ double s_rate[64];
+    const int k = blockIdx.y;
+    load_rates(s_rate, rates, k / L.nrhs, L.n);
+    __syncthreads();
+    uint32_t h;
+    if (!row_h(L, parity, h)) return;
+    const uint32_t v = state_of(h, parity);
+    const size_t o = (size_t)k * L.ld;
+    double acc = x0[(size_t)(k % L.nrhs) * x0_ld + v];
+    uint32_t g = Gx[v];
+    while (g) {
+        int i = __ffs(g) - 1;
+        g &= g - 1;
+        uint32_t u = v ^ (1u << i);
+        // u has the other parity; its half index is u >> 1
+        const double zu = (parity ? ZE : ZO)[o + (u >> 1)];
+        acc += s_rate[2 * i + ((u >> i) & 1u)] * zu;
+    }
+    if (direct) {
+        const uint32_t* Fh = parity ? L.F1 : L.F0;
+        Zout[o + h] = acc / out_rate(s_rate, Fh[h], v);
+    } else {
+        b[o + h] = acc;
+    }
+}
+
+__global__ void k_group_store(Layout L, int parity, const double* __restrict__ src, double* __restrict__ dst) {
+    const int k = blockIdx.y;
+    uint32_t h;
+    if (!row_h(L, parity, h)) return;
+    dst[(size_t)k * L.ld + h] = src[(size_t)k * L.ld + h];
+}
+
+// copy system rows j -> idx[j] (K' systems) between half-layout arrays
+__global__ void k_scatter_systems(size_t ld, const int32_t* __restrict__ idx, const double* __restrict__ src,
+                                  double* __restrict__ dst) {
+    const int j = blockIdx.y;
+    size_t h = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= ld) return;
+    dst[(size_t)idx[j] * ld + h] = src[(size_t)j * ld + h];
+}
+
+// Block forward solve of K systems (rate set k / nrhs, x0 row k % nrhs); results in
+// the half-layout arrays ZE (even) and ZO (odd).
+int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, int nrhs, const double* rates,
+                        const double* x0, size_t x0_ld, double* ZE, double* ZO, const esl_solve_opts& o,
+                        SolveOut& out) {
+    cudaStream_t s = ctx->stream;
+    BlockPlan* P = nullptr;
+    ESL_TRY(get_plan(ctx, net, P));
+    const uint32_t H = (uint32_t)(net->N / 2);
+    Layout L;
+    L.n = net->n;
+    L.H = H;
+    L.ld = ((size_t)H + 31) & ~(size_t)31;
+    L.nrhs = nrhs;
+    L.M0 = P->hm.get();
+    L.M1 = P->hm.get() + H;
+    L.F0 = P->hm.get() + 2 * (size_t)H;
+    L.F1 = P->hm.get() + 3 * (size_t)H;
+    L.pins = nullptr;
+    L.term_of = nullptr;
+    L.T = 0;
+    L.act = nullptr;
+    int st_ = ESL_OK;
+    const size_t vec = (size_t)K * L.ld;
+    double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
+    double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
+    if (st_ != ESL_OK) return st_;
+    esl_solve_opts go = o;
+    go.method = ESL_METHOD_FP64;
+    go.d_warm = nullptr;
+    const int G = (int)P->max_scc.size();
+    for (int gi = 0; gi < G; gi++) {
+        L.list0 = P->list0.get() + P->off0[gi];
+        L.list1 = P->list1.get() + P->off1[gi];
+        L.n0 = P->off0[gi + 1] - P->off0[gi];
+        L.n1 = P->off1[gi + 1] - P->off1[gi];
+        const int direct = P->max_scc[gi] == 1;
+        if (L.n0)
+            k_group_rhs<<<grid_rows(L, 0, K), kT, 0, s>>>(L, 0, rates, x0, x0_ld, P->Gx.get(), ZE, ZO, bE, direct,
+                                                          ZE);
+        if (L.n1)
+            k_group_rhs<<<grid_rows(L, 1, K), kT, 0, s>>>(L, 1, rates, x0, x0_ld, P->Gx.get(), ZE, ZO, bO, direct,
+                                                          ZO);
+        ESL_CUDA(cudaGetLastError());
+        if (direct) continue;
+        double *x64 = nullptr, *zE = nullptr;
+        SolveOut so;
+        int rc = krylov_solve<true>(ctx, ws, L, rates, K, bE, bO, nullptr, 0, go, x64, zE, so);
+        if (debug_enabled())
+            fprintf(stderr, "[esl] group %d/%d even %u odd %u max_scc %d: rc %d iters %d relres %.3e\n", gi, G, L.n0,
+                    L.n1, P->max_scc[gi], rc, so.iters, so.relres);
+        out.iters += so.iters;
+        if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
+        if (L.n0) k_group_store<<<grid_rows(L, 0, K), kT, 0, s>>>(L, 0, zE, ZE);
+        if (L.n1) k_group_store<<<grid_rows(L, 1, K), kT, 0, s>>>(L, 1, x64, ZO);
+        ESL_CUDA(cudaGetLastError());
+        double worst = 0.0;
+        if (rc == ESL_ERR_NOT_CONVERGED) {
+            // LU fallback for the systems that missed the budget
+            std::vector<int32_t> failed;
+            for (int k = 0; k < K; k++)
+                if (so.sys_relres[k] > kAcceptRel) failed.push_back(k);
+                else worst = std::max(worst, so.sys_relres[k]);
+            const int nscc = (int)(P->off_scc[gi + 1] - P->off_scc[gi]);
+            const bool covered = P->max_scc[gi] <= kDenseFallbackMax;
+            if (!covered || nscc == 0) {
+                out.converged = false;
+                worst = so.relres;
+            } else {
+                const int Kf = (int)failed.size();
+                std::vector<int64_t> scr(nscc);
+                int64_t acc = 0;
+                for (int jj = 0; jj < nscc; jj++) {
+                    scr[jj] = acc;
+                    int64_t sz = 0;
+                    ESL_CUDA(cudaMemcpyAsync(&sz, P->scc_size.get() + P->off_scc[gi] + jj, 4, cudaMemcpyDeviceToHost, s));
+                    ESL_CUDA(cudaStreamSynchronize(s));
+                    acc += sz * (sz + 1);
+                }
+                int64_t* d_scr = (int64_t*)ws.get(S_LUOFF, (size_t)nscc * 8, &st_);
+                int32_t* d_sys = (int32_t*)ws.get(S_LUSYS, (size_t)Kf * 4, &st_);
+                double* scratch = (double*)ws.get(S_LU, (size_t)acc * Kf * 8, &st_);
+                if (st_ != ESL_OK) return st_;
+                ESL_CUDA(cudaMemcpyAsync(d_scr, scr.data(), (size_t)nscc * 8, cudaMemcpyHostToDevice, s));
+                ESL_CUDA(cudaMemcpyAsync(d_sys, failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
+                k_dense_block<<<dim3((unsigned)nscc, (unsigned)Kf), 256, 0, s>>>(
+                    net->n, P->scc_beg.get() + P->off_scc[gi], P->scc_size.get() + P->off_scc[gi], d_scr, d_sys, acc,
+                    net->order.get(), net->F.get(), net->G.get(), rates, nrhs, L.ld, bE, bO, ZE, ZO, scratch);
+                ESL_CUDA(cudaGetLastError());
+                ESL_CUDA(cudaStreamSynchronize(s));
+                if (debug_enabled())
+                    fprintf(stderr, "[esl] group %d: dense LU fallback for %d systems on %d SCC blocks\n", gi, Kf, nscc);
+            }
+        } else {
+            worst = so.relres;
+        }
+        out.relres = std::max(out.relres, worst);
+    }
+    if (!out.converged) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "block solve: relative residual %.3e above tolerance", out.relres);
         return fail(ESL_ERR_NOT_CONVERGED, msg);
     }
     return ESL_OK;
@@ -1028,6 +1501,9 @@ int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const 
     L.pins = nullptr;
     L.term_of = nullptr;
     L.T = 0;
+    L.act = nullptr;
+    L.list0 = L.list1 = nullptr;
+    L.n0 = L.n1 = 0;
     return ESL_OK;
 }
 
@@ -1047,10 +1523,8 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         o.d_warm = nullptr;
     }
     if (o.tol <= 0) o.tol = 1e-10;
-    if (o.max_iters <= 0) o.max_iters = 2000;
+    if (o.max_iters <= 0) o.max_iters = 600;
     if (o.max_refine <= 0) o.max_refine = 6;
-    if (o.method == ESL_METHOD_DIRECT)
-        return fail(ESL_ERR_INVALID, "ESL_METHOD_DIRECT is not available in this build");
     if (!ctx->work) ctx->work = new Workspace();
     Workspace& ws = *static_cast<Workspace*>(ctx->work);
     cudaStream_t s = ctx->stream;
@@ -1119,6 +1593,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             to.tol = std::min(o.tol, 1e-12);
             to.d_warm = nullptr;
             to.max_refine = std::max(o.max_refine, 8);
+            to.max_iters = std::max(o.max_iters, 5000);
             double *x64 = nullptr, *zE = nullptr;
             SolveOut so;
             ESL_TRY(krylov_solve<true>(ctx, ws, L, d_rates, B, bE, bO, nullptr, 0, to, x64, zE, so));
@@ -1143,23 +1618,79 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         Layout L;
         ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, true, L, R));
         const size_t vec = (size_t)K * L.ld;
-        double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
-        double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
-        if (st_ != ESL_OK) return st_;
-        dim3 g = grid2(L.H, K);
-        k_rhs<true><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
-        ESL_CUDA(cudaGetLastError());
-        double *x64 = nullptr, *zE = nullptr;
+        double* ZE = nullptr;
+        double* ZO = nullptr;
+        int rc = ESL_OK;
         SolveOut so;
-        int rc = krylov_solve<true>(ctx, ws, L, d_rates, K, bE, bO, o.d_warm, N, o, x64, zE, so);
-        agg.iters += so.iters;
-        agg.refinements = so.refinements;
-        agg.relres = so.relres;
-        agg.converged = so.converged;
+        if (o.method == ESL_METHOD_DIRECT) {
+            ZE = (double*)ws.get(S_ZEF, vec * 8, &st_);
+            ZO = (double*)ws.get(S_ZOF, vec * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            esl_solve_opts bo = o;
+            bo.max_iters = std::max(o.max_iters, kBlockBudget);
+            rc = block_forward_solve(ctx, ws, net, K, R, d_rates, d_x0, N, ZE, ZO, bo, so);
+            agg.iters += so.iters;
+            agg.relres = so.relres;
+            agg.converged = so.converged;
+        } else {
+            double* bE = (double*)ws.get(S_BE, vec * 8, &st_);
+            double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            dim3 g = grid2(L.H, K);
+            k_rhs<true><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
+            ESL_CUDA(cudaGetLastError());
+            double *x64 = nullptr, *zE = nullptr;
+            rc = krylov_solve<true>(ctx, ws, L, d_rates, K, bE, bO, o.d_warm, N, o, x64, zE, so);
+            agg.iters += so.iters;
+            agg.refinements = so.refinements;
+            agg.relres = so.relres;
+            agg.converged = so.converged;
+            // keep the whole-system result out of the Krylov scratch slots
+            ws.swap(S_X64, S_ZOF);
+            ws.swap(S_ZE, S_ZEF);
+            ZO = x64;
+            ZE = zE;
+            if (rc == ESL_ERR_NOT_CONVERGED) {
+                // fallback: systems that missed the budget go through the block solve
+                std::vector<int32_t> failed;
+                for (int k = 0; k < K; k++)
+                    if (so.sys_relres[k] > kAcceptRel) failed.push_back(k);
+                const int Kf = (int)failed.size();
+                if (debug_enabled()) fprintf(stderr, "[esl] block-solve fallback for %d of %d systems\n", Kf, K);
+                double* r_sub = (double*)ws.get(S_RSUB, (size_t)Kf * 2 * n * 8, &st_);
+                double* x_sub = (double*)ws.get(S_XSUB, (size_t)Kf * N * 8, &st_);
+                int32_t* d_failed = (int32_t*)ws.get(S_LIST, (size_t)Kf * 4, &st_);
+                double* ZEb = (double*)ws.get(S_ZEB, (size_t)Kf * L.ld * 8, &st_);
+                double* ZOb = (double*)ws.get(S_ZOB, (size_t)Kf * L.ld * 8, &st_);
+                if (st_ != ESL_OK) return st_;
+                for (int j = 0; j < Kf; j++) {
+                    const int k = failed[j];
+                    ESL_CUDA(cudaMemcpyAsync(r_sub + (size_t)j * 2 * n, d_rates + (size_t)(k / R) * 2 * n, 2 * n * 8,
+                                             cudaMemcpyDeviceToDevice, s));
+                    ESL_CUDA(cudaMemcpyAsync(x_sub + (size_t)j * N, d_x0 + (size_t)(k % R) * N, N * 8,
+                                             cudaMemcpyDeviceToDevice, s));
+                }
+                ESL_CUDA(cudaMemcpyAsync(d_failed, failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
+                esl_solve_opts bo = o;
+                bo.max_iters = std::max(o.max_iters, kBlockBudget);
+                SolveOut sb;
+                rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
+                agg.iters += sb.iters;
+                agg.converged = sb.converged;
+                double worst = 0.0;
+                for (int k = 0; k < K; k++)
+                    if (so.sys_relres[k] <= kAcceptRel) worst = std::max(worst, so.sys_relres[k]);
+                agg.relres = std::max(worst, sb.relres);
+                dim3 gs((unsigned)((L.ld + 255) / 256), (unsigned)Kf);
+                k_scatter_systems<<<gs, 256, 0, s>>>(L.ld, d_failed, ZEb, ZE);
+                k_scatter_systems<<<gs, 256, 0, s>>>(L.ld, d_failed, ZOb, ZO);
+                ESL_CUDA(cudaGetLastError());
+            }
+        }
         if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
         k_terminal_mass<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, L.ld, d_rates, d_x0, N,
                                                                     net->order.get(), net->term_of.get(),
-                                                                    net->G.get(), zE, x64, y);
+                                                                    net->G.get(), ZE, ZO, y);
         ESL_CUDA(cudaGetLastError());
         if (rc == ESL_ERR_NOT_CONVERGED) {
             if (rep) {
@@ -1200,6 +1731,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             SolveOut so;
             esl_solve_opts lo = o;
             lo.d_warm = nullptr;
+            lo.max_iters = std::max(o.max_iters, 5000);
             ESL_TRY(krylov_solve<false>(ctx, ws, L, d_rates, T, bE, bO, nullptr, 0, lo, x64, zE, so));
             k_scatter_L<<<g, kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), zE, x64, d_L);
             ESL_CUDA(cudaGetLastError());

@@ -156,7 +156,7 @@ def test_solver_toy_goldens(esl, ctx, goldens, name, method):
     np.testing.assert_allclose(val, c["nonzero_data_each"], atol=1e-12, rtol=0)
 
 
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", [0, 1, 2])
 @pytest.mark.parametrize("name", ["solver.kras", "solver.mammal", "rates.toy", "zero_rate.toy", "solver.cohen",
                                   "symbolic.cohen_rates"])
 def test_solver_goldens(esl, ctx, goldens, name, method):
@@ -180,7 +180,7 @@ def test_solver_goldens(esl, ctx, goldens, name, method):
     np.testing.assert_allclose(res.marginals.cpu().numpy(), om_marg, atol=1e-9, rtol=0)
 
 
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", [0, 1, 2])
 def test_random_networks_vs_oracle(esl, ctx, method):
     for name, text in _nets():
         om = O.Model(text=text)
@@ -231,7 +231,7 @@ def test_large_terminal_scc(esl, ctx):
     np.testing.assert_allclose(res.x_inf.cpu().numpy(), expect, atol=1e-12, rtol=0)
 
 
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", [0, 1, 2])
 def test_batch_vs_oracle(esl, ctx, method):
     w = synth.config_batch(seed=5, n_networks=3, n_rate_sets=4, n_x0=3, n_lo=9, n_hi=12)
     for net_g, rates, x0s in zip(w.networks, w.rates, w.x0):
