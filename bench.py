@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Benchmark: stationary distributions per second on the n=20 precision network x 512
+held-out rate sets (the learned-warm-start workload's held-out sweep).
+
+One step = the whole hot path for one batch: bit-sliced transition table, SCC /
+levels / reordering, terminal kernels, transient solve and x_inf + marginals for
+512 (rate set, x0) pairs, inputs resident in HBM.  `value` = solves/s over all
+ranks (max device time over ranks); `e2e` = the same through the public Python API
+with pinned host inputs copied in and the results (marginals + terminal-state
+probabilities, i.e. every nonzero of x_inf) copied back inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--method fp64|mixed|direct]
+    python bench.py --impl reference ...   # the CPU FP64 oracle on the host cores
+
+Synthetic data: seeded random network (paraexastolog_b200.synth), no dataset.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+from paraexastolog_b200 import synth  # noqa: E402
+
+METRIC = "solves/s, n=20 x 512 rate sets, learned+mixed vs FP64 sparse LU at L1<=1e-9"
+BATCH = 512
+
+
+def workload(rank: int):
+    w = synth.config_learned(n_rate_sets=4096)
+    net = w.networks[0]
+    rates = w.rates[0][-BATCH:]
+    if rank > 0:  # weak scaling: further seeded rate sets of the same distribution
+        rng = np.random.default_rng(10_000 + rank)
+        rates = synth.log_uniform_rates(rng, net.n, BATCH)
+    return net, np.ascontiguousarray(rates), np.ascontiguousarray(w.x0[0])
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_byte():
+    """DRAM bytes per algorithmic byte of the Schur operator from the committed ncu
+    capture summary (profiles/schur_operator_traffic.json), or None."""
+    path = os.path.join(REPO, "profiles", "schur_operator_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get("dram_bytes_per_algorithmic_byte")
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    import torch.distributed as dist
+
+    import paraexastolog_b200 as esl
+
+    torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
+    ctx = esl.Context(device, stream)
+    net_g, rates, x0 = workload(rank)
+    method = {"fp64": esl.METHOD_FP64, "mixed": esl.METHOD_MIXED, "direct": esl.METHOD_DIRECT}[args.method]
+    model = esl.Model.parse(net_g.bnet)
+    d_rates = torch.tensor(rates, device=f"cuda:{device}")
+    d_x0 = torch.tensor(x0, device=f"cuda:{device}")
+    N = 1 << model.n
+
+    def step():
+        net = esl.Net.build(ctx, model, rates[0])
+        res = esl.solve_batch(ctx, net, d_rates, d_x0, method=method, tol=args.tol)
+        return net, res
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    for _ in range(args.warmup):
+        net, res = step()
+    # device-resident timed region
+    barrier()
+    launches0 = esl.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(device) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            net, res = step()
+        e1.record(stream)
+        barrier()
+    launches = esl.launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    iters, relres = res.report.iterations, res.report.relres
+
+    # roofline of the dominant kernel pair (Schur operator) from live CUDA events
+    ctx.set_profiling(True)
+    for _ in range(max(1, min(args.steps, 2))):
+        step()
+    op_ms, op_bytes, op_launches = ctx.profile()
+    ctx.set_profiling(False)
+
+    # end to end through the public API: pinned host inputs, results back to host
+    h_rates = torch.tensor(rates).pin_memory()
+    h_x0 = torch.tensor(x0).pin_memory()
+    term_idx = None
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h2d = d2h = 0
+    f0.record(stream)
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        m = esl.Model.parse(net_g.bnet)
+        dr = h_rates.to(f"cuda:{device}", non_blocking=True)
+        dx = h_x0.to(f"cuda:{device}", non_blocking=True)
+        h2d = dr.numel() * 8 + dx.numel() * 8
+        net = esl.Net.build(ctx, m, rates[0])
+        res = esl.solve_batch(ctx, net, dr, dx, method=method, tol=args.tol)
+        if term_idx is None:
+            order, _, _, _ = net.export()
+            term_idx = order[: net.terminal_states].long()
+        probs = res.x_inf[:, 0, :].index_select(1, term_idx).cpu()
+        marg = res.marginals.cpu()
+        d2h = probs.numel() * 8 + marg.numel() * 8
+    f1.record(stream)
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    e2e_wall = time.perf_counter() - t_wall
+
+    t = torch.tensor([ms, e2e_ms, float(launches)], device=f"cuda:{device}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    out = None
+    if rank == 0:
+        solves = BATCH * args.steps * world
+        peak, peak_kind = peaks()
+        achieved = op_bytes / (op_ms * 1e-3) / 1e9 if op_ms > 0 else None
+        tpb = traffic_per_byte()
+        out = {
+            "metric": METRIC,
+            "value": solves / (ms * 1e-3),
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.method != "mixed" else "f32+f64",
+            "data": "synthetic (seeded random Boolean network, log-uniform rates)",
+            "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "n_nodes": model.n,
+                       "states": N, "batch_rate_sets": BATCH, "initial_distributions": 1,
+                       "method": args.method, "tol_relres": args.tol,
+                       "l2": "working set > L2 (x_inf alone is 4 GB per step)",
+                       "parallelism": f"replicas x{world} (rate-set shards)",
+                       "step": "table + SCC/levels/order + terminal kernels + transient solve + x_inf/marginals"},
+            "e2e": {"value": solves / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "wall_s": e2e_wall},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "schur_operator (k_elim + k_apply)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
+                         "peak_kind": peak_kind,
+                         "traffic": (op_bytes / op_launches) * tpb if (tpb and op_launches) else None,
+                         "algorithmic_bytes_per_launch": op_bytes / op_launches if op_launches else None,
+                         "launches": op_launches},
+            "solver": {"iterations": iters, "relres": relres},
+            "clocks": clocks,
+        }
+    return out
+
+
+def cpu_baseline(sample: int):
+    """The CPU FP64 oracle on this host's cores over a bounded sample of rate sets."""
+    import oracle as O
+
+    net_g, rates, x0 = workload(0)
+    m = O.Model(text=net_g.bnet)
+    sym = m.analyse(rates[0])
+    threads = min(os.cpu_count() or 1, sample)
+    r = rates[:sample]
+    xs = np.broadcast_to(x0, (sample, x0.size)).copy()
+    t = time.perf_counter()
+    sym.solve_many(r, xs, threads=threads)
+    dt = time.perf_counter() - t
+    return {"value": sample / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} of the 512 held-out rate sets, oracle symbolic analysis excluded"}, dt
+
+
+def run_reference(args):
+    sample = max(8, min(os.cpu_count() or 8, 32))
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(sample)
+    total, solves = 0.0, 0
+    for _ in range(args.steps):
+        cb, dt = cpu_baseline(sample)
+        total += dt
+        solves += sample
+    value = solves / total
+    cb["value"] = value
+    return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "sample_per_step": sample},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--method", default="direct", choices=["direct", "fp64", "mixed"])
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    out = run_ours(args, rank, world, local)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"], _ = cpu_baseline(max(8, min(os.cpu_count() or 8, 16)))
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

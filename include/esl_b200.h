@@ -38,15 +38,17 @@ typedef struct esl_model esl_model; /* parsed bnet: node names + DNF clauses */
 typedef struct esl_net esl_net;     /* device symbolic data for one (model, zero-rate pattern) */
 
 /* Solver method for the transient absorption and large terminal kernels. */
-#define ESL_METHOD_FP64 0    /* FP64 BiCGStab on the red-black reduced system */
-#define ESL_METHOD_MIXED 1   /* FP32 BiCGStab + FP64 iterative refinement */
-#define ESL_METHOD_DIRECT 2  /* FP64 block-triangular LU (dense per SCC block); small blocks only */
+#define ESL_METHOD_FP64 0    /* FP64 BiCGStab on the red-black reduced system of all transient states;
+                                systems that miss the budget fall back to ESL_METHOD_DIRECT */
+#define ESL_METHOD_MIXED 1   /* as FP64 with FP32 inner iterations and FP64 iterative refinement */
+#define ESL_METHOD_DIRECT 2  /* block forward substitution over SCC levels: singleton levels exact,
+                                other levels FP64 Krylov with a dense-LU fallback per SCC block */
 
 typedef struct esl_solve_opts {
     int method;            /* ESL_METHOD_* */
     double tol;            /* relative residual target of the transient solve (default 1e-10) */
-    int max_iters;         /* iteration budget per Krylov solve (default 2000) */
-    int max_refine;        /* FP64 refinement steps for ESL_METHOD_MIXED (default 4) */
+    int max_iters;         /* Krylov iteration budget per system before the fallback (default 600) */
+    int max_refine;        /* FP64 refinement steps (default 6) */
     const double* d_warm;  /* optional warm start of the occupation vector, B x N (device), or NULL */
 } esl_solve_opts;
 
@@ -134,6 +136,16 @@ int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rat
  * results copied back to host buffers.  Builds and frees its own net. */
 int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,
                    double* x_inf, double* marginals, const esl_solve_opts* opts, esl_report* report);
+
+/* ---- measurement hook (no counterpart in the reference): when on, the solver
+ *      records CUDA events around every application of the reduced (Schur) operator
+ *      in its Krylov loop.  esl_ctx_profile returns the summed device time, the
+ *      algorithmic bytes (each array touched once per launch) and the launch count
+ *      since profiling was switched on. */
+int esl_ctx_set_profiling(esl_ctx* ctx, int on);
+int esl_ctx_profile(esl_ctx* ctx, double* total_ms, double* total_bytes, int* launches);
+/* number of kernels this library has launched in this process (no counterpart in the reference) */
+int esl_launch_count(uint64_t* count);
 
 #ifdef __cplusplus
 }

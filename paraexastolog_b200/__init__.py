@@ -68,6 +68,9 @@ def lib():
     L.esl_ctx_create.argtypes = [C.c_int, vp, P(vp)]
     L.esl_ctx_destroy.argtypes = [vp]
     L.esl_ctx_synchronize.argtypes = [vp]
+    L.esl_ctx_set_profiling.argtypes = [vp, C.c_int]
+    L.esl_launch_count.argtypes = [P(C.c_uint64)]
+    L.esl_ctx_profile.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_int)]
     L.esl_model_load.argtypes = [cp, P(vp)]
     L.esl_model_parse.argtypes = [cp, P(vp)]
     L.esl_model_free.argtypes = [vp]
@@ -93,6 +96,13 @@ def lib():
     L.esl_solve_host.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    c = C.c_uint64()
+    check(lib().esl_launch_count(C.byref(c)))
+    return c.value
 
 
 def check(code: int):
@@ -145,6 +155,16 @@ class Context:
 
     def synchronize(self):
         check(lib().esl_ctx_synchronize(self._h))
+
+    def set_profiling(self, on: bool):
+        """Record CUDA events around each reduced-operator application of the solver."""
+        check(lib().esl_ctx_set_profiling(self._h, int(bool(on))))
+
+    def profile(self):
+        """(summed device ms, algorithmic bytes, launches) since profiling was switched on."""
+        ms, by, n = C.c_double(), C.c_double(), C.c_int()
+        check(lib().esl_ctx_profile(self._h, C.byref(ms), C.byref(by), C.byref(n)))
+        return ms.value, by.value, n.value
 
 
 class Model:

@@ -1,6 +1,7 @@
 // C ABI of the library (declarations and reference citations in include/esl_b200.h).
 #include <cub/device/device_scan.cuh>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -12,6 +13,9 @@
 namespace esl {
 
 static thread_local std::string g_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -85,6 +89,12 @@ extern "C" {
 const char* esl_last_error(void) { return g_error.c_str(); }
 int esl_version(void) { return 100; }
 
+int esl_launch_count(uint64_t* count) {
+    if (!count) return fail(ESL_ERR_INVALID, "NULL argument");
+    *count = g_launches.load();
+    return ESL_OK;
+}
+
 int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out) {
     if (!out) return fail(ESL_ERR_INVALID, "out is NULL");
     *out = nullptr;
@@ -116,10 +126,36 @@ int esl_ctx_destroy(esl_ctx* c) {
     if (!c) return ESL_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->work) free_workspace(c->work);
+    for (auto e : c->prof_pool) cudaEventDestroy(e);
     c->d_flag.release();
     if (c->h_flag) cudaFreeHost(c->h_flag);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
+    return ESL_OK;
+}
+
+int esl_ctx_set_profiling(esl_ctx* c, int on) {
+    if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
+    ESL_CUDA(cudaStreamSynchronize(c->stream));
+    c->prof = on != 0;
+    c->prof_recs.clear();
+    c->prof_used = 0;
+    return ESL_OK;
+}
+
+int esl_ctx_profile(esl_ctx* c, double* total_ms, double* total_bytes, int* launches) {
+    if (!c || !total_ms || !total_bytes || !launches) return fail(ESL_ERR_INVALID, "NULL argument");
+    ESL_CUDA(cudaStreamSynchronize(c->stream));
+    double ms = 0.0, bytes = 0.0;
+    for (auto& r : c->prof_recs) {
+        float t = 0.f;
+        ESL_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        ms += t;
+        bytes += r.bytes;
+    }
+    *total_ms = ms;
+    *total_bytes = bytes;
+    *launches = (int)c->prof_recs.size();
     return ESL_OK;
 }
 
@@ -268,6 +304,7 @@ int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char*
         p_fixed = fixed_probability / (double)match;
         p_other = match == N ? 0.0 : (1.0 - fixed_probability) / (double)(N - match);
     }
+    ESL_COUNT_LAUNCH();
     k_initial_state<<<(unsigned)((N + 255) / 256), 256, 0, ctx->stream>>>(N, mask, val, p_fixed, p_other, d_x0);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;

@@ -28,6 +28,10 @@ int fail(int code, const std::string& msg);
         if (s_ != ESL_OK) return s_;   \
     } while (0)
 
+// ---- launch accounting: every kernel launch of the library is counted --------
+void count_launch();
+#define ESL_COUNT_LAUNCH() ::esl::count_launch()
+
 // ---- host model -------------------------------------------------------------
 struct Clause {
     uint32_t pos, neg;
@@ -80,6 +84,23 @@ struct esl_ctx {
     uint32_t* h_flag = nullptr;       // pinned host scratch for fixpoint flags
     esl::DevBuf<unsigned long long> d_flag;  // device counters (8 slots)
     void* work = nullptr;             // solver workspace (grow-only), freed with the context
+    // measurement hook: events around Schur-operator applications
+    bool prof = false;
+    struct ProfRec {
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> prof_pool;
+    size_t prof_used = 0;
+    cudaEvent_t prof_event() {
+        if (prof_used == prof_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            prof_pool.push_back(e);
+        }
+        return prof_pool[prof_used++];
+    }
 };
 
 struct esl_model {

@@ -274,12 +274,14 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     DevBuf<uint8_t> reached;
     ESL_TRY(color.alloc(N));
     ESL_TRY(reached.alloc(N));
+    ESL_COUNT_LAUNCH();
     k_fill<<<nb, kThreads, 0, s>>>(N, lab, -1);
     ESL_CUDA(cudaGetLastError());
     ESL_TRY(fl.reset());
 
     auto trim = [&]() -> int {
         return fixpoint(fl, [&]() -> int {
+            ESL_COUNT_LAUNCH();
             k_trim<<<nb, kThreads, 0, s>>>(n, N, F, G, lab, ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
@@ -291,20 +293,25 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     int64_t rounds = 0;
     while (st[1] < N) {
         if (++rounds > (int64_t)N) return fail(ESL_ERR_TIMEOUT, "SCC colouring rounds exceeded");
+        ESL_COUNT_LAUNCH();
         k_color_init<<<nb, kThreads, 0, s>>>(N, lab, color.get(), reached.get());
         ESL_CUDA(cudaGetLastError());
         ESL_TRY(fixpoint(fl, [&]() -> int {
+            ESL_COUNT_LAUNCH();
             k_color_fw<<<nb, kThreads, 0, s>>>(N, G, lab, color.get(), ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         }, 4, budget, "forward colouring"));
+        ESL_COUNT_LAUNCH();
         k_root_init<<<nb, kThreads, 0, s>>>(N, lab, color.get(), reached.get());
         ESL_CUDA(cudaGetLastError());
         ESL_TRY(fixpoint(fl, [&]() -> int {
+            ESL_COUNT_LAUNCH();
             k_reach_bw<<<nb, kThreads, 0, s>>>(N, F, lab, color.get(), reached.get(), ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         }, 4, budget, "backward reach"));
+        ESL_COUNT_LAUNCH();
         k_assign<<<nb, kThreads, 0, s>>>(N, lab, color.get(), reached.get(), ctx->d_flag.get());
         ESL_CUDA(cudaGetLastError());
         ESL_TRY(trim());
@@ -312,16 +319,21 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     }
     // canonical labels: smallest state of each SCC
     ESL_TRY(canon.alloc(N));
+    ESL_COUNT_LAUNCH();
     k_fill<<<nb, kThreads, 0, s>>>(N, canon.get(), 0x7FFFFFFF);
+    ESL_COUNT_LAUNCH();
     k_canon_min<<<nb, kThreads, 0, s>>>(N, lab, canon.get());
+    ESL_COUNT_LAUNCH();
     k_canon_apply<<<nb, kThreads, 0, s>>>(N, lab, canon.get());
     ESL_CUDA(cudaGetLastError());
 
     // levels (indexed by label)
     ESL_TRY(level.alloc(N));
+    ESL_COUNT_LAUNCH();
     k_fill<<<nb, kThreads, 0, s>>>(N, level.get(), 0);
     ESL_CUDA(cudaGetLastError());
     ESL_TRY(fixpoint(fl, [&]() -> int {
+        ESL_COUNT_LAUNCH();
         k_level<<<nb, kThreads, 0, s>>>(N, F, lab, level.get(), ctx->d_flag.get());
         ESL_CUDA(cudaGetLastError());
         return ESL_OK;
@@ -336,6 +348,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         ESL_TRY(keys_out.alloc(N));
         ESL_TRY(vals.alloc(N));
         ESL_TRY(net->order.alloc(N));
+        ESL_COUNT_LAUNCH();
         k_keys<<<nb, kThreads, 0, s>>>(N, lab, level.get(), keys.get(), vals.get());
         ESL_CUDA(cudaGetLastError());
         size_t tmp_bytes = 0;
@@ -348,6 +361,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         // SCC heads
         ESL_TRY(pos.alloc(N));
         ESL_TRY(head.alloc(N));
+        ESL_COUNT_LAUNCH();
         k_heads<<<nb, kThreads, 0, s>>>(N, keys_out.get(), pos.get(), head.get());
         ESL_CUDA(cudaGetLastError());
         DevBuf<int32_t> offs;
@@ -370,6 +384,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         int32_t Nend = (int32_t)N;
         ESL_CUDA(cudaMemcpyAsync(net->offsets.get() + n_sccs, &Nend, sizeof(int32_t), cudaMemcpyHostToDevice, s));
         ESL_TRY(net->levels.alloc(n_sccs));
+        ESL_COUNT_LAUNCH();
         k_scc_levels<<<(unsigned)((n_sccs + kThreads - 1) / kThreads), kThreads, 0, s>>>(
             (int)n_sccs, net->offsets.get(), net->order.get(), lab, level.get(), net->levels.get());
         ESL_CUDA(cudaGetLastError());
@@ -390,11 +405,13 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
             net->max_terminal = std::max(net->max_terminal, net->h_offsets[t + 1] - net->h_offsets[t]);
     }
     ESL_TRY(net->term_of.alloc(N));
+    ESL_COUNT_LAUNCH();
     k_term_of<<<nb, kThreads, 0, s>>>(N, net->T, net->term_states, net->offsets.get(), net->order.get(),
                                       net->term_of.get());
     ESL_CUDA(cudaGetLastError());
     ESL_TRY(net->Fdom.alloc(N));
     ESL_TRY(net->Gdom.alloc(N));
+    ESL_COUNT_LAUNCH();
     k_domain_masks<<<nb, kThreads, 0, s>>>(n, N, F, G, net->term_of.get(), net->Fdom.get(), net->Gdom.get());
     ESL_CUDA(cudaGetLastError());
     ESL_CUDA(cudaStreamSynchronize(s));

@@ -861,18 +861,29 @@ inline dim3 grid_rows(const Layout& L, int parity, int K) {
     return dim3((std::max(rows, 1u) + kT - 1) / kT, (unsigned)K);
 }
 
+// Algorithmic bytes of one Schur-operator application (k_elim + k_apply) over K
+// systems: every array once -- elim reads x (odd) and writes w (even); apply reads
+// x, w, r0 and writes y (odd); the four mask words per half index are shared by
+// all systems.
+double schur_bytes(const Layout& L, int K, size_t tsz) {
+    const double n0 = L.list0 ? L.n0 : L.H, n1 = L.list1 ? L.n1 : L.H;
+    return (double)K * tsz * (2.0 * n0 + 4.0 * n1) + 8.0 * (n0 + n1);
+}
+
 template <bool FWD, class T>
 int inner_bicgstab(esl_ctx* ctx, Layout L, const double* rates, int K, const double* dS, const double* r64,
                    KState* st, int* n_active, int32_t* act, InnerVecs<T> iv, int max_iters, int* iters_out) {
     cudaStream_t s = ctx->stream;
     unsigned sb = (unsigned)((K + 127) / 128);
     L.act = nullptr;
+    ESL_COUNT_LAUNCH();
     k_inner_start<T><<<grid_rows(L, 1, K), kT, 0, s>>>(L, r64, iv.r, iv.r0, iv.d, iv.ph, iv.v, st);
     int it = 0;
     const int check_every = 8;
     while (it < max_iters) {
         // launch only over the systems still running
         ESL_CUDA(cudaMemsetAsync(n_active, 0, sizeof(int), s));
+        ESL_COUNT_LAUNCH();
         k_active_list<<<sb, 128, 0, s>>>(K, st, n_active, act);
         int active = 0;
         ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -881,15 +892,35 @@ int inner_bicgstab(esl_ctx* ctx, Layout L, const double* rates, int K, const dou
         L.act = act;
         const dim3 g0 = grid_rows(L, 0, active), g1 = grid_rows(L, 1, active);
         for (int c = 0; c < check_every; c++, it++) {
+            ESL_COUNT_LAUNCH();
             k_update_p<T><<<g1, kT, 0, s>>>(L, dS, iv.r, iv.ph, iv.v, st);
+            cudaEvent_t ea = nullptr, eb = nullptr;
+            if (ctx->prof) {
+                ea = ctx->prof_event();
+                eb = ctx->prof_event();
+                cudaEventRecord(ea, s);
+            }
+            ESL_COUNT_LAUNCH();
             k_elim<FWD, T, T><<<g0, kT, 0, s>>>(L, rates, iv.ph, nullptr, iv.w, st);
+            ESL_COUNT_LAUNCH();
             k_apply<FWD, 0, T, T><<<g1, kT, 0, s>>>(L, rates, iv.ph, iv.w, dS, nullptr, iv.r0, iv.v, st);
+            if (ctx->prof) {
+                cudaEventRecord(eb, s);
+                ctx->prof_recs.push_back({ea, eb, schur_bytes(L, active, sizeof(T))});
+            }
+            ESL_COUNT_LAUNCH();
             k_scal_alpha<<<sb, 128, 0, s>>>(K, st);
+            ESL_COUNT_LAUNCH();
             k_update_s<T><<<g1, kT, 0, s>>>(L, dS, iv.r, iv.v, iv.sh, st);
+            ESL_COUNT_LAUNCH();
             k_elim<FWD, T, T><<<g0, kT, 0, s>>>(L, rates, iv.sh, nullptr, iv.w, st);
+            ESL_COUNT_LAUNCH();
             k_apply<FWD, 2, T, T><<<g1, kT, 0, s>>>(L, rates, iv.sh, iv.w, dS, nullptr, nullptr, iv.t, st);
+            ESL_COUNT_LAUNCH();
             k_scal_omega<<<sb, 128, 0, s>>>(K, st);
+            ESL_COUNT_LAUNCH();
             k_update_xr<T><<<g1, kT, 0, s>>>(L, dS, iv.d, iv.r, iv.r0, iv.ph, iv.sh, iv.t, st);
+            ESL_COUNT_LAUNCH();
             k_scal_beta<<<sb, 128, 0, s>>>(K, st, max_iters);
         }
         ESL_CUDA(cudaGetLastError());
@@ -973,16 +1004,23 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     const dim3 g0 = grid_rows(L, 0, K), g1 = grid_rows(L, 1, K);
     unsigned sb = (unsigned)((K + 127) / 128);
     ESL_CUDA(cudaMemsetAsync(st, 0, (size_t)K * sizeof(KState), s));
+    ESL_COUNT_LAUNCH();
     k_schur_diag<FWD><<<g1, kT, 0, s>>>(L, rates, dS);
     // reduced rhs: bS = bO + A_oe (bE / q_e)
+    ESL_COUNT_LAUNCH();
     k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, (const double*)nullptr, bE, w64, nullptr);
+    ESL_COUNT_LAUNCH();
     k_apply<FWD, 4, double, double><<<g1, kT, 0, s>>>(L, rates, (const double*)nullptr, w64, dS, bO, nullptr, bS,
                                                       nullptr);
+    ESL_COUNT_LAUNCH();
     k_norm2<<<g1, kT, 0, s>>>(L, bS, st);
-    if (warm)
+    if (warm) {
+        ESL_COUNT_LAUNCH();
         k_half_from_full<<<g1, kT, 0, s>>>(L, warm, warm_ld, x64);
-    else
+    } else {
+        ESL_COUNT_LAUNCH();
         k_zero_rows<<<g1, kT, 0, s>>>(L, 1, x64);
+    }
     ESL_CUDA(cudaGetLastError());
     const double tol = o.tol > 0 ? o.tol : 1e-10;
     // FP32 inner solves stop at 1e-4 relative: below that the FP32 operator's
@@ -995,14 +1033,18 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
     double* rt = (double*)ws.get(S_RT, vec * 8, &st_);
     if (st_ != ESL_OK) return st_;
     // true residual of the starting iterate
+    ESL_COUNT_LAUNCH();
     k_zero_r<<<sb, 128, 0, s>>>(K, st);
+    ESL_COUNT_LAUNCH();
     k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, x64, nullptr, w64, nullptr);
+    ESL_COUNT_LAUNCH();
     k_apply<FWD, 3, double, double><<<g1, kT, 0, s>>>(L, rates, x64, w64, dS, bS, nullptr, r64, st);
     for (;; outer++) {
         ESL_CUDA(cudaMemsetAsync(n_active, 0, 2 * sizeof(int), s));
         // inner target: a relative reduction that reaches tol in one inner solve,
         // but not below what the inner precision can deliver
         const double floor_now = inner64 ? 1e-13 : floor_rel;
+        ESL_COUNT_LAUNCH();
         k_outer_check<<<sb, 128, 0, s>>>(K, st, tol * tol, floor_now * floor_now, outer, o.max_iters, n_active);
         ESL_CUDA(cudaGetLastError());
         ESL_CUDA(cudaMemcpyAsync(&active, n_active, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1020,26 +1062,34 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
             }
         }
         if (active == 0 || outer >= o.max_refine) break;
+        ESL_COUNT_LAUNCH();
         k_mark_inner<<<sb, 128, 0, s>>>(K, st);
         int it = 0;
+        ESL_COUNT_LAUNCH();
         k_zero_trial<<<sb, 128, 0, s>>>(K, st);
         if (!inner64) {
             InnerVecs<float> iv{(float*)iv_p[0], (float*)iv_p[1], (float*)iv_p[2], (float*)iv_p[3],
                                 (float*)iv_p[4], (float*)iv_p[5], (float*)iv_p[6], (float*)iv_p[7]};
             ESL_TRY((inner_bicgstab<FWD, float>(ctx, L, rates, K, dS, r64, st, n_active, act, iv, o.max_iters, &it)));
+            ESL_COUNT_LAUNCH();
             k_trial<float><<<g1, kT, 0, s>>>(L, x64, iv.d, xt, st);
         } else {
             InnerVecs<double> iv{(double*)iv_p[0], (double*)iv_p[1], (double*)iv_p[2], (double*)iv_p[3],
                                  (double*)iv_p[4], (double*)iv_p[5], (double*)iv_p[6], (double*)iv_p[7]};
             ESL_TRY((inner_bicgstab<FWD, double>(ctx, L, rates, K, dS, r64, st, n_active, act, iv, o.max_iters, &it)));
+            ESL_COUNT_LAUNCH();
             k_trial<double><<<g1, kT, 0, s>>>(L, x64, iv.d, xt, st);
         }
         total_iters += it;
         // true residual of the trial iterate; commit where it improved
+        ESL_COUNT_LAUNCH();
         k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, xt, nullptr, w64, nullptr);
+        ESL_COUNT_LAUNCH();
         k_apply<FWD, 5, double, double><<<g1, kT, 0, s>>>(L, rates, xt, w64, dS, bS, nullptr, rt, st);
         ESL_CUDA(cudaMemsetAsync(n_active + 1, 0, sizeof(int), s));
+        ESL_COUNT_LAUNCH();
         k_commit_flags<<<sb, 128, 0, s>>>(K, st, n_active + 1);
+        ESL_COUNT_LAUNCH();
         k_commit<<<g1, kT, 0, s>>>(L, x64, r64, xt, rt, st);
         ESL_CUDA(cudaGetLastError());
         int noimp = 0;
@@ -1049,6 +1099,7 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
         if (noimp > 0 && !inner64) inner64 = true;
     }
     // even half: zE = (bE + A_eo x) / q_e
+    ESL_COUNT_LAUNCH();
     k_elim<FWD, double, double><<<g0, kT, 0, s>>>(L, rates, x64, bE, zE, nullptr);
     ESL_CUDA(cudaGetLastError());
     std::vector<KState> h_st(K);
@@ -1305,6 +1356,7 @@ int get_plan(esl_ctx* ctx, const esl_net* net, BlockPlan*& out) {
     if (rc == ESL_OK) {
         if (!l0.empty()) chk(cudaMemcpyAsync(P->list0.get(), l0.data(), l0.size() * 4, cudaMemcpyHostToDevice, s));
         if (!l1.empty()) chk(cudaMemcpyAsync(P->list1.get(), l1.data(), l1.size() * 4, cudaMemcpyHostToDevice, s));
+        ESL_COUNT_LAUNCH();
         k_scc_masks<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(net->n, N, net->F.get(), net->G.get(),
                                                                 net->labels.get(), net->term_of.get(), P->Gx.get(),
                                                                 P->hm.get(), H);
@@ -1408,12 +1460,16 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
         L.n0 = P->off0[gi + 1] - P->off0[gi];
         L.n1 = P->off1[gi + 1] - P->off1[gi];
         const int direct = P->max_scc[gi] == 1;
-        if (L.n0)
+        if (L.n0) {
+            ESL_COUNT_LAUNCH();
             k_group_rhs<<<grid_rows(L, 0, K), kT, 0, s>>>(L, 0, rates, x0, x0_ld, P->Gx.get(), ZE, ZO, bE, direct,
                                                           ZE);
-        if (L.n1)
+        }
+        if (L.n1) {
+            ESL_COUNT_LAUNCH();
             k_group_rhs<<<grid_rows(L, 1, K), kT, 0, s>>>(L, 1, rates, x0, x0_ld, P->Gx.get(), ZE, ZO, bO, direct,
                                                           ZO);
+        }
         ESL_CUDA(cudaGetLastError());
         if (direct) continue;
         double *x64 = nullptr, *zE = nullptr;
@@ -1424,8 +1480,8 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
                     L.n1, P->max_scc[gi], rc, so.iters, so.relres);
         out.iters += so.iters;
         if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
-        if (L.n0) k_group_store<<<grid_rows(L, 0, K), kT, 0, s>>>(L, 0, zE, ZE);
-        if (L.n1) k_group_store<<<grid_rows(L, 1, K), kT, 0, s>>>(L, 1, x64, ZO);
+        if (L.n0) { ESL_COUNT_LAUNCH(); k_group_store<<<grid_rows(L, 0, K), kT, 0, s>>>(L, 0, zE, ZE); }
+        if (L.n1) { ESL_COUNT_LAUNCH(); k_group_store<<<grid_rows(L, 1, K), kT, 0, s>>>(L, 1, x64, ZO); }
         ESL_CUDA(cudaGetLastError());
         double worst = 0.0;
         if (rc == ESL_ERR_NOT_CONVERGED) {
@@ -1456,6 +1512,7 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
                 if (st_ != ESL_OK) return st_;
                 ESL_CUDA(cudaMemcpyAsync(d_scr, scr.data(), (size_t)nscc * 8, cudaMemcpyHostToDevice, s));
                 ESL_CUDA(cudaMemcpyAsync(d_sys, failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
+                ESL_COUNT_LAUNCH();
                 k_dense_block<<<dim3((unsigned)nscc, (unsigned)Kf), 256, 0, s>>>(
                     net->n, P->scc_beg.get() + P->off_scc[gi], P->scc_size.get() + P->off_scc[gi], d_scr, d_sys, acc,
                     net->order.get(), net->F.get(), net->G.get(), rates, nrhs, L.ld, bE, bO, ZE, ZO, scratch);
@@ -1486,6 +1543,7 @@ int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const 
     uint32_t* M1 = M0 + H;
     uint32_t* F0 = M0 + 2 * (size_t)H;
     uint32_t* F1 = M0 + 3 * (size_t)H;
+    ESL_COUNT_LAUNCH();
     k_half_masks<<<(H + kT - 1) / kT, kT, 0, ctx->stream>>>(net->n, H, fwd ? net->Gdom.get() : net->Fdom.get(),
                                                            net->F.get(), net->term_of.get(), big_term, dom, M0, M1,
                                                            F0, F1);
@@ -1543,6 +1601,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             if (sz >= 2 && sz <= kDenseTerm) dense_list.push_back(t);
             if (sz > kDenseTerm) big_list.push_back(t);
         }
+        ESL_COUNT_LAUNCH();
         k_unit_terminals<<<dim3((T + 127) / 128, B), 128, 0, s>>>(T, net->offsets.get(), TS, Rb);
         ESL_CUDA(cudaGetLastError());
         if (!dense_list.empty()) {
@@ -1553,6 +1612,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             for (int t : dense_list) smax = std::max(smax, net->h_offsets[t + 1] - net->h_offsets[t]);
             size_t smem = (size_t)smax * (smax + 1) * 8 + (size_t)smax * 4 + 16;
             ESL_CUDA(cudaFuncSetAttribute(k_dense_terminal, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ESL_COUNT_LAUNCH();
             k_dense_terminal<<<dim3((unsigned)dense_list.size(), B), 256, smem, s>>>(
                 n, d_list, net->offsets.get(), net->order.get(), net->F.get(), d_rates, TS, Rb);
             ESL_CUDA(cudaGetLastError());
@@ -1569,8 +1629,10 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_CUDA(cudaMemcpyAsync(d_big, h_big.data(), T, cudaMemcpyHostToDevice, s));
             ESL_CUDA(cudaMemsetAsync(d_best, 0, (size_t)B * T * 8, s));
             dim3 gt((TS + kT - 1) / kT, B);
+            ESL_COUNT_LAUNCH();
             k_pin_score<<<gt, kT, 0, s>>>(n, T, TS, net->order.get(), net->term_of.get(), d_big, net->F.get(),
                                           net->G.get(), d_rates, d_best);
+            ESL_COUNT_LAUNCH();
             k_pin_decode<<<(unsigned)((B * T + 255) / 256), 256, 0, s>>>(B * T, d_best, d_pins);
             ESL_CUDA(cudaGetLastError());
             Layout L;
@@ -1584,6 +1646,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             double* sums = (double*)ws.get(S_SUM, (size_t)B * T * 8, &st_);
             if (st_ != ESL_OK) return st_;
             dim3 g = grid2(L.H, B);
+            ESL_COUNT_LAUNCH();
             k_rhs_pinned<<<g, kT, 0, s>>>(L, d_rates, net->G.get(), bE, bO);
             ESL_CUDA(cudaGetLastError());
             // terminal kernels are solved in FP64 throughout: they can be badly
@@ -1599,8 +1662,10 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_TRY(krylov_solve<true>(ctx, ws, L, d_rates, B, bE, bO, nullptr, 0, to, x64, zE, so));
             agg.iters += so.iters;
             ESL_CUDA(cudaMemsetAsync(sums, 0, (size_t)B * T * 8, s));
+            ESL_COUNT_LAUNCH();
             k_pinned_sum<<<gt, kT, 0, s>>>(T, net->offsets.get(), net->order.get(), d_big, d_pins, L.ld, zE, x64, TS,
                                            Rb, sums);
+            ESL_COUNT_LAUNCH();
             k_pinned_norm<<<gt, kT, 0, s>>>(T, net->offsets.get(), d_big, TS, Rb, sums);
             ESL_CUDA(cudaGetLastError());
             ESL_CUDA(cudaStreamSynchronize(s));
@@ -1637,6 +1702,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
             if (st_ != ESL_OK) return st_;
             dim3 g = grid2(L.H, K);
+            ESL_COUNT_LAUNCH();
             k_rhs<true><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
             ESL_CUDA(cudaGetLastError());
             double *x64 = nullptr, *zE = nullptr;
@@ -1682,12 +1748,15 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
                     if (so.sys_relres[k] <= kAcceptRel) worst = std::max(worst, so.sys_relres[k]);
                 agg.relres = std::max(worst, sb.relres);
                 dim3 gs((unsigned)((L.ld + 255) / 256), (unsigned)Kf);
+                ESL_COUNT_LAUNCH();
                 k_scatter_systems<<<gs, 256, 0, s>>>(L.ld, d_failed, ZEb, ZE);
+                ESL_COUNT_LAUNCH();
                 k_scatter_systems<<<gs, 256, 0, s>>>(L.ld, d_failed, ZOb, ZO);
                 ESL_CUDA(cudaGetLastError());
             }
         }
         if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
+        ESL_COUNT_LAUNCH();
         k_terminal_mass<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, L.ld, d_rates, d_x0, N,
                                                                     net->order.get(), net->term_of.get(),
                                                                     net->G.get(), ZE, ZO, y);
@@ -1703,6 +1772,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         }
     } else {
         dim3 g((TS + 127) / 128, K);
+        ESL_COUNT_LAUNCH();
         k_terminal_mass<<<g, 128, 0, s>>>(n, T, TS, R, 0, d_rates, d_x0, N, net->order.get(), net->term_of.get(),
                                           net->G.get(), nullptr, nullptr, y);
         ESL_CUDA(cudaGetLastError());
@@ -1711,6 +1781,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     if (d_x_inf) {
         ESL_CUDA(cudaMemsetAsync(d_x_inf, 0, (size_t)K * N * 8, s));
         if (d_marg) ESL_CUDA(cudaMemsetAsync(d_marg, 0, (size_t)K * n * 8, s));
+        ESL_COUNT_LAUNCH();
         k_scatter_xinf<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, N, net->order.get(),
                                                                    net->term_of.get(), Rb, y, d_x_inf, d_marg);
         ESL_CUDA(cudaGetLastError());
@@ -1725,6 +1796,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             double* bO = (double*)ws.get(S_BO, vec * 8, &st_);
             if (st_ != ESL_OK) return st_;
             dim3 g = grid2(L.H, T);
+            ESL_COUNT_LAUNCH();
             k_rhs<false><<<g, kT, 0, s>>>(L, n, d_rates, d_x0, N, net->F.get(), net->term_of.get(), bE, bO);
             ESL_CUDA(cudaGetLastError());
             double *x64 = nullptr, *zE = nullptr;
@@ -1733,6 +1805,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             lo.d_warm = nullptr;
             lo.max_iters = std::max(o.max_iters, 5000);
             ESL_TRY(krylov_solve<false>(ctx, ws, L, d_rates, T, bE, bO, nullptr, 0, lo, x64, zE, so));
+            ESL_COUNT_LAUNCH();
             k_scatter_L<<<g, kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), zE, x64, d_L);
             ESL_CUDA(cudaGetLastError());
         } else {
@@ -1742,6 +1815,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, false, L, T));
             double* z = (double*)ws.get(S_BE, (size_t)T * L.ld * 8 * 2, &st_);
             if (st_ != ESL_OK) return st_;
+            ESL_COUNT_LAUNCH();
             k_scatter_L<<<grid2(L.H, T), kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), z, z + (size_t)T * L.ld,
                                                     d_L);
             ESL_CUDA(cudaGetLastError());

@@ -267,6 +267,7 @@ int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* bl
     uint64_t N = 1ull << dm.n;
     uint64_t words = (N + 31) / 32;
     int64_t blocks = flip_mask_blocks(dm.n);
+    ESL_COUNT_LAUNCH();
     k_flip_masks<<<(unsigned)blocks, kMaskThreads, 0, s>>>(dm, words, N, F, G, block_counts);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
@@ -276,12 +277,16 @@ int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl
                     int32_t* cols, int64_t nnz, cudaStream_t s) {
     uint64_t N = 1ull << n;
     int64_t blocks = flip_mask_blocks(n);
-    if (n <= 16)
+    if (n <= 16) {
+        ESL_COUNT_LAUNCH();
         k_emit_csc<16><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
-    else if (n <= 24)
+    } else if (n <= 24) {
+        ESL_COUNT_LAUNCH();
         k_emit_csc<24><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
-    else
+    } else {
+        ESL_COUNT_LAUNCH();
         k_emit_csc<30><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+    }
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
 }
@@ -290,8 +295,10 @@ int masks_from_csc(int n, const int32_t* indptr, const int32_t* rows, uint32_t* 
                    unsigned long long* d_bad, cudaStream_t s) {
     uint64_t N = 1ull << n;
     unsigned blocks = (unsigned)((N + 255) / 256);
+    ESL_COUNT_LAUNCH();
     k_masks_from_csc<<<blocks, 256, 0, s>>>(n, N, indptr, rows, F, d_bad);
     ESL_CUDA(cudaGetLastError());
+    ESL_COUNT_LAUNCH();
     k_in_masks<<<blocks, 256, 0, s>>>(n, N, F, G);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
