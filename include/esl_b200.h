@@ -101,6 +101,29 @@ int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32
 /* per-state flip masks: bit i of d_out[s] = edge s -> s^(1<<i); of d_in[s] = edge s^(1<<i) -> s */
 int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in);
 
+/* ---- allocation-free transition table.  No counterpart in the reference: the
+ *      reference allocates its work arrays in every stage.
+ *      For callers that must not allocate device memory while they run: code
+ *      inside a framework whose caching allocator already holds the GPU's memory,
+ *      loops that cannot afford the device-wide synchronisation of cudaFree, and
+ *      services that allocate only at start-up.  Output is the same CSC as
+ *      esl_table_build (d_indptr[N+1], d_rows/d_cols with rows_capacity entries,
+ *      d_cols may be NULL), on the given stream of the CURRENT device.  It takes no
+ *      context and calls no cudaMalloc/cudaFree: its scratch (~4.2 MB) is a static
+ *      device array that every GPU loading the library keeps until exit.
+ *      Limits: at most ESL_STATIC_TABLE_MAX_NODES nodes and
+ *      ESL_STATIC_TABLE_MAX_CLAUSES DNF clauses, else ESL_ERR_TOO_LARGE; *nnz
+ *      always receives the edge count once it is known, and a table with more than
+ *      rows_capacity edges returns ESL_ERR_TOO_LARGE without writing the arrays.
+ *      The first call on a device looks up the array's device address; make that
+ *      first call before any stream capture.  All calls on a device share the
+ *      array: calls whose GPU work overlaps race, so serialise them.
+ *      Synchronises the stream before returning. */
+#define ESL_STATIC_TABLE_MAX_NODES 20
+#define ESL_STATIC_TABLE_MAX_CLAUSES 8192
+int esl_table_build_static(const esl_model* m, const double* rates, void* cuda_stream, int32_t* d_indptr,
+                           int32_t* d_rows, int32_t* d_cols, int64_t rows_capacity, int64_t* nnz);
+
 /* ---- transition graph: replaces transition_graph::reorganize_vertices
  *      (cuda/src/transition_graph.cu:39-202, kernels/transition_graph.cu:3-52).
  *      Builds table masks, SCCs, terminal SCCs, levels and the reordering on the device. */

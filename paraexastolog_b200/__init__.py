@@ -85,6 +85,7 @@ def lib():
     L.esl_table_nnz.argtypes = [vp, vp, vp, P(C.c_int64)]
     L.esl_table_build.argtypes = [vp, vp, vp, vp, vp, vp]
     L.esl_flip_masks.argtypes = [vp, vp, vp, vp, vp]
+    L.esl_table_build_static.argtypes = [vp, vp, vp, vp, vp, vp, C.c_int64, P(C.c_int64)]
     L.esl_net_build.argtypes = [vp, vp, vp, P(vp)]
     L.esl_net_from_csc.argtypes = [vp, C.c_int, vp, vp, P(vp)]
     L.esl_net_free.argtypes = [vp]
