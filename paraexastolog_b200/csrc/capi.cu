@@ -114,7 +114,9 @@ int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out) {
         c->own_stream = true;
     }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
-    if (cudaMallocHost(&c->h_flag, 64) != cudaSuccess || c->d_flag.alloc(8) != ESL_OK) {
+    if (cudaMallocHost(&c->h_flag, 64) != cudaSuccess || c->d_flag.alloc(8) != ESL_OK ||
+        cudaEventCreateWithFlags(&c->poll_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming) != cudaSuccess) {
         esl_ctx_destroy(c);
         return fail(ESL_ERR_NOMEM, "context allocation failed");
     }
@@ -126,6 +128,9 @@ int esl_ctx_destroy(esl_ctx* c) {
     if (!c) return ESL_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->work) free_workspace(c->work);
+    if (c->sweep_work) free_sweep_workspace(c->sweep_work);
+    for (auto e : c->poll_ev)
+        if (e) cudaEventDestroy(e);
     for (auto e : c->prof_pool) cudaEventDestroy(e);
     c->d_flag.release();
     if (c->h_flag) cudaFreeHost(c->h_flag);

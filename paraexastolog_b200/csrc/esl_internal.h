@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,36 @@ struct DevBuf {
     T* get() const { return p; }
 };
 
+// Grow-only device workspace kept in the context between calls.
+struct Workspace {
+    std::vector<std::pair<void*, size_t>> bufs;
+    void* get(int slot, size_t bytes, int* status) {
+        if ((int)bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
+        auto& b = bufs[slot];
+        if (b.second < bytes) {
+            if (b.first) cudaFree(b.first);
+            b.first = nullptr;
+            b.second = 0;
+            if (cudaMalloc(&b.first, bytes) != cudaSuccess) {
+                b.first = nullptr;
+                *status = fail(ESL_ERR_NOMEM, "workspace allocation of " + std::to_string(bytes) + " bytes failed");
+                return nullptr;
+            }
+            b.second = bytes;
+        }
+        return b.first;
+    }
+    void swap(int a, int b) {
+        int m = std::max(a, b);
+        if ((int)bufs.size() <= m) bufs.resize(m + 1, {nullptr, 0});
+        std::swap(bufs[a], bufs[b]);
+    }
+    ~Workspace() {
+        for (auto& b : bufs)
+            if (b.first) cudaFree(b.first);
+    }
+};
+
 }  // namespace esl
 
 // ---- public handles -------------------------------------------------------------
@@ -84,6 +115,8 @@ struct esl_ctx {
     uint32_t* h_flag = nullptr;       // pinned host scratch for fixpoint flags
     esl::DevBuf<unsigned long long> d_flag;  // device counters (8 slots)
     void* work = nullptr;             // solver workspace (grow-only), freed with the context
+    void* sweep_work = nullptr;       // level-sweep workspace (grow-only), freed with the context
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // convergence polls of the level sweep
     // measurement hook: events around Schur-operator applications
     bool prof = false;
     struct ProfRec {
@@ -125,8 +158,12 @@ struct esl_net {
     // level-group plan of the block forward solve, built on first use
     void* plan = nullptr;
     void (*plan_free)(void*) = nullptr;
+    // slot plan of the state-major level sweep, built on first use
+    void* sweep = nullptr;
+    void (*sweep_free)(void*) = nullptr;
     ~esl_net() {
         if (plan && plan_free) plan_free(plan);
+        if (sweep && sweep_free) sweep_free(sweep);
     }
 };
 
@@ -154,6 +191,20 @@ int build_graph(esl_ctx* ctx, esl_net* net);
 
 // solve.cu
 void free_workspace(void* w);
+
+// sweep.cu: state-major level sweep of the transient forward solve.  Adds into
+// y[k * T + t] the mass that terminal SCC t receives in system k (rate set k / nrhs,
+// x0 row k % nrhs).  Systems that miss the tolerance are listed in `failed` (their y
+// rows are left as computed) and the call returns ESL_ERR_NOT_CONVERGED.
+struct SweepStats {
+    int iters = 0, refinements = 0, dense_groups = 0, krylov_groups = 0;
+    double relres = 0.0;
+    std::vector<int32_t> failed;
+};
+bool sweep_supported(const esl_net* net);
+int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
+                  size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st);
+void free_sweep_workspace(void* w);
 int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                 double* d_x_inf, double* d_marg, double* d_R, double* d_L, const esl_solve_opts* opts,
                 esl_report* rep);

@@ -931,36 +931,6 @@ int inner_bicgstab(esl_ctx* ctx, Layout L, const double* rates, int K, const dou
 
 }  // namespace
 
-// Grow-only device workspace kept in the context between calls.
-struct Workspace {
-    std::vector<std::pair<void*, size_t>> bufs;
-    void* get(int slot, size_t bytes, int* status) {
-        if ((int)bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
-        auto& b = bufs[slot];
-        if (b.second < bytes) {
-            if (b.first) cudaFree(b.first);
-            b.first = nullptr;
-            b.second = 0;
-            if (cudaMalloc(&b.first, bytes) != cudaSuccess) {
-                b.first = nullptr;
-                *status = fail(ESL_ERR_NOMEM, "workspace allocation of " + std::to_string(bytes) + " bytes failed");
-                return nullptr;
-            }
-            b.second = bytes;
-        }
-        return b.first;
-    }
-    void swap(int a, int b) {
-        int m = std::max(a, b);
-        if ((int)bufs.size() <= m) bufs.resize(m + 1, {nullptr, 0});
-        std::swap(bufs[a], bufs[b]);
-    }
-    ~Workspace() {
-        for (auto& b : bufs)
-            if (b.first) cudaFree(b.first);
-    }
-};
-
 void free_workspace(void* w) { delete static_cast<Workspace*>(w); }
 
 namespace {
@@ -1414,6 +1384,14 @@ __global__ void k_group_store(Layout L, int parity, const double* __restrict__ s
     dst[(size_t)k * L.ld + h] = src[(size_t)k * L.ld + h];
 }
 
+// dst row idx[j] = src row j (rows of `width` doubles)
+__global__ void k_set_rows(int width, const int32_t* __restrict__ idx, const double* __restrict__ src,
+                           double* __restrict__ dst) {
+    const int j = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < width) dst[(size_t)idx[j] * width + c] = src[(size_t)j * width + c];
+}
+
 // copy system rows j -> idx[j] (K' systems) between half-layout arrays
 __global__ void k_scatter_systems(size_t ld, const int32_t* __restrict__ idx, const double* __restrict__ src,
                                   double* __restrict__ dst) {
@@ -1679,7 +1657,69 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     if (st_ != ESL_OK) return st_;
     ESL_CUDA(cudaMemsetAsync(y, 0, (size_t)K * T * 8, s));
     const bool has_transient = (size_t)TS < N;
-    if (has_transient) {
+    bool swept = false;
+    if (has_transient && (o.method == ESL_METHOD_DIRECT || o.method == ESL_METHOD_MIXED) && sweep_supported(net)) {
+        // state-major level sweep; systems it cannot bring below the acceptance
+        // residual are redone by the block solve with its dense-LU fallback
+        SweepStats sw;
+        int rc = sweep_forward(ctx, net, K, R, d_rates, d_x0, N, o, y, sw);
+        agg.iters += sw.iters;
+        agg.relres = sw.relres;
+        if (rc == ESL_ERR_NOT_CONVERGED && !sw.failed.empty()) {
+            const int Kf = (int)sw.failed.size();
+            if (debug_enabled()) fprintf(stderr, "[esl] sweep: block-solve fallback for %d of %d systems\n", Kf, K);
+            Layout L;
+            ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, true, L, 1));
+            double* r_sub = (double*)ws.get(S_RSUB, (size_t)Kf * 2 * n * 8, &st_);
+            double* x_sub = (double*)ws.get(S_XSUB, (size_t)Kf * N * 8, &st_);
+            int32_t* d_failed = (int32_t*)ws.get(S_LIST, (size_t)Kf * 4, &st_);
+            double* ZEb = (double*)ws.get(S_ZEB, (size_t)Kf * L.ld * 8, &st_);
+            double* ZOb = (double*)ws.get(S_ZOB, (size_t)Kf * L.ld * 8, &st_);
+            double* y_sub = (double*)ws.get(S_SUM, (size_t)Kf * T * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            for (int j = 0; j < Kf; j++) {
+                const int k = sw.failed[j];
+                ESL_CUDA(cudaMemcpyAsync(r_sub + (size_t)j * 2 * n, d_rates + (size_t)(k / R) * 2 * n, 2 * n * 8,
+                                         cudaMemcpyDeviceToDevice, s));
+                ESL_CUDA(cudaMemcpyAsync(x_sub + (size_t)j * N, d_x0 + (size_t)(k % R) * N, N * 8,
+                                         cudaMemcpyDeviceToDevice, s));
+            }
+            ESL_CUDA(cudaMemcpyAsync(d_failed, sw.failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
+            esl_solve_opts bo = o;
+            bo.method = ESL_METHOD_DIRECT;
+            bo.d_warm = nullptr;
+            bo.max_iters = std::max(o.max_iters, kBlockBudget);
+            SolveOut sb;
+            rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
+            if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
+            agg.iters += sb.iters;
+            agg.converged = sb.converged;
+            agg.relres = std::max(agg.relres, sb.relres);
+            ESL_CUDA(cudaMemsetAsync(y_sub, 0, (size_t)Kf * T * 8, s));
+            ESL_COUNT_LAUNCH();
+            k_terminal_mass<<<dim3((TS + 127) / 128, Kf), 128, 0, s>>>(n, T, TS, 1, L.ld, r_sub, x_sub, N,
+                                                                         net->order.get(), net->term_of.get(),
+                                                                         net->G.get(), ZEb, ZOb, y_sub);
+            ESL_COUNT_LAUNCH();
+            k_set_rows<<<dim3((T + 127) / 128, Kf), 128, 0, s>>>(T, d_failed, y_sub, y);
+            ESL_CUDA(cudaGetLastError());
+            if (rc == ESL_ERR_NOT_CONVERGED) {
+                if (rep) {
+                    rep->iterations = agg.iters;
+                    rep->refinements = agg.refinements;
+                    rep->relres = agg.relres;
+                    rep->converged = 0;
+                }
+                return rc;
+            }
+        } else if (rc != ESL_OK) {
+            return rc;
+        }
+        swept = true;
+    }
+    if (swept) {
+        // terminal masses are in y
+    } else if (has_transient) {
         Layout L;
         ESL_TRY(make_layout(ctx, ws, net, 0, nullptr, true, L, R));
         const size_t vec = (size_t)K * L.ld;
