@@ -12,14 +12,13 @@
 // own level.  Level groups are solved one after another, sources first, and inside a
 // group every SCC is an independent diagonal block.  Per group:
 //   - singleton SCCs only: z_v = b_v / q_v;
-//   - SCCs of at most kSwDenseMax states: dense FP64 Gauss-Jordan per (SCC, system),
-//     without pivoting (a transient SCC leaks, so its block is column diagonally
-//     dominant);
 //   - otherwise BiCGStab on the odd-parity Schur complement.  Every edge flips one bit, so
 //     the graph is bipartite by popcount parity and the even rows are eliminated exactly.
 //     The right preconditioner is the Schur diagonal, and inner iterations run in FP64
 //     (ESL_METHOD_DIRECT) or FP32 (ESL_METHOD_MIXED) inside FP64 iterative refinement on
-//     the true residual.
+//     the true residual.  Groups whose SCCs all have at most kSwLocalMax states run the
+//     whole refinement inside one CTA per (SCC, 32 systems) (k_sw_local: block
+//     reductions, no grid-wide step); larger groups run one grid-wide kernel per step.
 //
 // Layout: every vector is [row][system], the Kp (K rounded up to 32) systems of a row
 // contiguous.  A warp handles 32 systems of one state, so every neighbour gather reads a
@@ -32,6 +31,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "esl_internal.h"
@@ -40,8 +40,8 @@ namespace esl {
 namespace {
 
 constexpr int kSwT = 256;            // threads per row kernel
-constexpr int kSwDenseMax = 256;     // largest SCC of a group solved by dense Gauss-Jordan
-constexpr int kSwDenseSmem = 160;    // dense SCCs up to this size keep their matrix in shared memory
+constexpr int kSwLocalMax = 512;     // largest SCC of a group solved CTA-locally
+constexpr int kSwLocalWarps = 16;    // most warps of a CTA-local solve
 constexpr int kSwPoll = 4;           // Krylov iterations launched between convergence polls
 constexpr double kSwAcceptRel = 1e-8;  // stagnating systems are accepted at this relative residual
 constexpr int kSwStall = 30;         // inner iterations without halving the residual before an inner solve stops
@@ -53,31 +53,30 @@ constexpr int SW_RUN = 4;    // runs an inner solve in this refinement step
 constexpr int SW_IDONE = 8;  // its inner solve has stopped
 
 // per-system scalar arrays (doubles), each Kp long
-enum Scal { C_BB, C_RR64, C_PREV, C_RHO, C_R0V, C_TS, C_TT, C_RR, C_RN, C_BETA, C_OMEGA, C_TARGET, C_BEST, C_NSCAL };
+enum Scal { C_BB, C_RR64, C_PREV, C_RHO, C_R0V, C_TS, C_TT, C_RR, C_RN, C_BETA, C_OMEGA, C_TARGET, C_BEST, C_SCALE,
+            C_NSCAL };
 // per-system int arrays
 enum IScal { I_FLAGS, I_ITERS, I_NOIMP, I_TOTAL, I_STALL, I_NISCAL };
 
 struct SwGroup {
     uint32_t beg, ne, no;  // first slot, even rows, odd rows
-    int kind;              // 0 singletons, 1 dense, 2 Krylov
+    int kind;              // 0 singletons, 1 CTA-local Krylov, 2 grid-wide Krylov
     int max_scc;
-    uint32_t scc0, nscc;   // dense groups: range in the dense SCC list
-    uint64_t scr;          // dense groups: scratch doubles per system (matrices kept in global memory)
-    int smax;              // dense groups: largest SCC
+    uint32_t scc0, nscc;   // local groups: range in the local SCC list (SCCs of >= 2 states)
+    int max_odd;           // local groups: most odd rows of one SCC
 };
 
 struct SweepPlan {
-    uint32_t M = 0, max_rows = 0, max_even = 0, max_odd = 0;
+    uint32_t M = 0, max_rows = 0, max_even = 0, max_odd = 0, max_even_local = 0, max_odd_local = 0;
     int TS = 0;
     std::vector<SwGroup> groups;
     DevBuf<uint2> rows;                  // per slot: (state, out-mask)
     DevBuf<uint32_t> ig_ptr, ig_ent;     // predecessors inside the group: slot << 5 | bit
     DevBuf<uint32_t> og_ptr, og_ent;     // predecessors in earlier groups
     DevBuf<uint32_t> tp_ptr, tp_ent;     // transient predecessors of terminal position p
-    DevBuf<uint32_t> dscc_off;           // dense SCCs: offsets into dscc_slots
-    DevBuf<uint32_t> dscc_slots;         // dense SCCs: slots, SCC by SCC
-    DevBuf<uint64_t> dscc_scr;           // dense SCCs: scratch offset within the group's per-system scratch
-    DevBuf<uint32_t> dloc;               // per slot of a dense group: index inside its SCC
+    DevBuf<uint32_t> lsc_off;            // local SCCs: offsets into lsc_slots
+    DevBuf<uint32_t> lsc_ne;             // local SCCs: number of even-parity slots (listed first)
+    DevBuf<uint32_t> lsc_slots;          // local SCCs: slots, SCC by SCC
 };
 
 void free_plan_sweep(void* p) { delete static_cast<SweepPlan*>(p); }
@@ -142,6 +141,37 @@ __device__ __forceinline__ bool sw_skip(const SwArgs& a, int k) {
     return !(f & SW_RUN) || (f & SW_IDONE);
 }
 
+// Sum over the predecessor entries ent[p0 .. p0 + cnt) of a row with state v of
+// rate(edge into v) * X[(entry >> 5) - base][k], added to acc in entry order.  All 32
+// lanes of a warp handle the same row (tiles are at least 32 systems wide), so the row's
+// entries (at most n <= 27) arrive in one coalesced load and are broadcast by shuffles,
+// and the gathers are issued four at a time.  Every lane of the warp must call it; lanes
+// with act == false load nothing.
+template <class TC, class TX>
+__device__ __forceinline__ TC sw_gather(const TC* s, const Tile& t, int Kp, uint32_t v,
+                                        const uint32_t* __restrict__ ent, uint32_t p0, int cnt,
+                                        const TX* __restrict__ X, uint32_t base, bool act, TC acc) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t mine = lane < cnt ? __ldg(ent + p0 + lane) : 0u;
+    int j = 0;
+    for (; j + 4 <= cnt; j += 4) {
+        uint32_t e[4];
+        TC x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) e[u] = __shfl_sync(0xffffffffu, mine, j + u);
+#pragma unroll
+        for (int u = 0; u < 4; u++) x[u] = act ? (TC)X[(size_t)((e[u] >> 5) - base) * Kp + t.k] : (TC)0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) acc += sw_in(s, v, (int)(e[u] & 31u), t) * x[u];
+    }
+    for (; j < cnt; j++) {
+        const uint32_t e = __shfl_sync(0xffffffffu, mine, j);
+        const TC x = act ? (TC)X[(size_t)((e >> 5) - base) * Kp + t.k] : (TC)0;
+        acc += sw_in(s, v, (int)(e & 31u), t) * x;
+    }
+    return acc;
+}
+
 // Block-wide sums of NV per-thread values for this thread's system, added atomically to
 // dst[j][k] by the first row-lane.
 template <int NV>
@@ -170,17 +200,17 @@ __global__ void __launch_bounds__(kSwT) k_sw_rhs(SwArgs a, const uint32_t* __res
     extern __shared__ double s_rate[];
     const Tile t = tile_of(a.KT);
     sw_rates(s_rate, a, t);
-    if (t.k >= a.K) return;
+    const bool act = t.k < a.K;
+    if (__all_sync(0xffffffffu, !act)) return;
     const uint32_t cnt = a.ne + a.no;
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < cnt; r += gridDim.x * t.RB) {
         const uint32_t slot = a.beg + r;
         const uint2 row = a.rows[slot];
         const uint32_t v = row.x;
-        double acc = x0[(size_t)(t.k % a.nrhs) * x0_ld + v];
-        for (uint32_t e = og_ptr[slot]; e < og_ptr[slot + 1]; e++) {
-            const uint32_t ent = og_ent[e];
-            acc += sw_in(s_rate, v, (int)(ent & 31u), t) * Z[(size_t)(ent >> 5) * a.Kp + t.k];
-        }
+        const uint32_t p0 = og_ptr[slot];
+        double acc = act ? x0[(size_t)(t.k % a.nrhs) * x0_ld + v] : 0.0;
+        acc = sw_gather<double, double>(s_rate, t, a.Kp, v, og_ent, p0, (int)(og_ptr[slot + 1] - p0), Z, 0u, act, acc);
+        if (!act) continue;
         if (DIRECT)
             Z[(size_t)slot * a.Kp + t.k] = acc / sw_q(s_rate, v, row.y, t);
         else
@@ -221,20 +251,19 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
     TC* s_rate = reinterpret_cast<TC*>(s_raw);
     const Tile t = tile_of(a.KT);
     sw_rates(s_rate, a, t);
-    if (sw_skip(a, t.k)) return;
+    const bool act = !sw_skip(a, t.k);
+    if (__all_sync(0xffffffffu, !act)) return;
     const uint32_t obase = a.beg + a.ne;
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne; r += gridDim.x * t.RB) {
         const uint32_t slot = a.beg + r;
         const uint2 row = a.rows[slot];
         const uint32_t v = row.x;
-        TC acc = C ? (TC)C[(size_t)r * a.Kp + t.k] : (TC)0;
+        TC acc = (C && act) ? (TC)C[(size_t)r * a.Kp + t.k] : (TC)0;
         if (X) {
-            for (uint32_t e = a.ig_ptr[slot]; e < a.ig_ptr[slot + 1]; e++) {
-                const uint32_t ent = a.ig_ent[e];
-                acc += sw_in(s_rate, v, (int)(ent & 31u), t) * (TC)X[(size_t)((ent >> 5) - obase) * a.Kp + t.k];
-            }
+            const uint32_t p0 = a.ig_ptr[slot];
+            acc = sw_gather<TC, TX>(s_rate, t, a.Kp, v, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, obase, act, acc);
         }
-        W[(size_t)r * a.Kp + t.k] = (TW)(acc / sw_q(s_rate, v, row.y, t));
+        if (act) W[(size_t)r * a.Kp + t.k] = (TW)(acc / sw_q(s_rate, v, row.y, t));
     }
 }
 
@@ -252,18 +281,17 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
     const Tile t = tile_of(a.KT);
     sw_rates(s_rate, a, t);
     double d0 = 0.0, d1 = 0.0;
-    const bool skip = (MODE >= 2) ? sw_skip(a, t.k) : (t.k >= a.K);
-    if (!skip) {
+    const bool act = !((MODE >= 2) ? sw_skip(a, t.k) : (t.k >= a.K));
+    if (__any_sync(0xffffffffu, act)) {
         for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
             const uint32_t slot = a.beg + a.ne + r;
             const uint2 row = a.rows[slot];
             const uint32_t o = row.x;
             const size_t idx = (size_t)r * a.Kp + t.k;
-            T flow = 0;
-            for (uint32_t e = a.ig_ptr[slot]; e < a.ig_ptr[slot + 1]; e++) {
-                const uint32_t ent = a.ig_ent[e];
-                flow += sw_in(s_rate, o, (int)(ent & 31u), t) * W[(size_t)((ent >> 5) - a.beg) * a.Kp + t.k];
-            }
+            const uint32_t p0 = a.ig_ptr[slot];
+            const T flow = sw_gather<T, T>(s_rate, t, a.Kp, o, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), W, a.beg,
+                                           act, (T)0);
+            if (!act) continue;
             if (MODE == 0) {
                 const double y = B[idx] + (double)flow;
                 Y[idx] = (T)y;
@@ -413,14 +441,17 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
             sc.i[I_FLAGS][k] = (rr <= accept2 * b2) ? SW_DONE : (SW_DONE | SW_FAIL);
             continue;
         }
+        // the inner solve works on the residual scaled to unit norm
+        const double scale = 1.0 / sqrt(rr);
         sc.i[I_FLAGS][k] = SW_RUN;
         sc.i[I_ITERS][k] = 0;
         sc.c[C_PREV][k] = rr;
-        sc.c[C_RHO][k] = rr;
+        sc.c[C_SCALE][k] = scale;
+        sc.c[C_RHO][k] = 1.0;
         sc.c[C_BETA][k] = 0.0;
         sc.c[C_OMEGA][k] = 1.0;
-        sc.c[C_TARGET][k] = fmax(inner_rel2 * rr, 0.01 * tol2 * b2);
-        sc.c[C_BEST][k] = rr;
+        sc.c[C_TARGET][k] = fmax(inner_rel2, 0.01 * tol2 * b2 * scale * scale);
+        sc.c[C_BEST][k] = 1.0;
         sc.i[I_STALL][k] = 0;
         sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = 0.0;
         cnt++;
@@ -430,16 +461,18 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
     if (threadIdx.x == 0) *active = s_cnt;
 }
 
-// start of an inner solve: R = R0 = (T) R64, D = PH = V = 0
+// start of an inner solve: R = R0 = (T) (R64 * scale), D = PH = V = 0
 template <class T>
-__global__ void __launch_bounds__(kSwT) k_sw_start(SwArgs a, const double* __restrict__ R64, T* __restrict__ R,
+__global__ void __launch_bounds__(kSwT) k_sw_start(SwArgs a, const double* __restrict__ scale,
+                                                   const double* __restrict__ R64, T* __restrict__ R,
                                                    T* __restrict__ R0, T* __restrict__ D, T* __restrict__ PH,
                                                    T* __restrict__ V) {
     const Tile t = tile_of(a.KT);
     if (sw_skip(a, t.k)) return;
+    const double sk = scale[t.k];
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
         const size_t idx = (size_t)r * a.Kp + t.k;
-        const T x = (T)R64[idx];
+        const T x = (T)(R64[idx] * sk);
         R[idx] = x;
         R0[idx] = x;
         D[idx] = 0;
@@ -449,82 +482,344 @@ __global__ void __launch_bounds__(kSwT) k_sw_start(SwArgs a, const double* __res
 }
 
 template <class T>
-__global__ void __launch_bounds__(kSwT) k_sw_commit(SwArgs a, const T* __restrict__ D, double* __restrict__ X64) {
+__global__ void __launch_bounds__(kSwT) k_sw_commit(SwArgs a, const double* __restrict__ scale,
+                                                    const T* __restrict__ D, double* __restrict__ X64) {
     const Tile t = tile_of(a.KT);
     if (t.k >= a.K || !(a.flags[t.k] & SW_RUN)) return;
+    const double nrm = 1.0 / scale[t.k];
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
         const size_t idx = (size_t)r * a.Kp + t.k;
-        X64[idx] += (double)D[idx];
+        X64[idx] += nrm * (double)D[idx];
     }
 }
 
-// starting iterate of the odd rows: the warm start (K x N, by state) or 0
-__global__ void __launch_bounds__(kSwT) k_sw_warm(SwArgs a, const double* __restrict__ warm, size_t warm_ld,
+// Starting iterate of the odd rows.  A row without in-group predecessors is a singleton
+// SCC: its value bS / dS is exact.  Other rows take the warm start (K x N, by state) or 0.
+__global__ void __launch_bounds__(kSwT) k_sw_init(SwArgs a, const double* __restrict__ warm, size_t warm_ld,
+                                                  const double* __restrict__ bS, const double* __restrict__ dS,
                                                   double* __restrict__ X64) {
     const Tile t = tile_of(a.KT);
     if (t.k >= a.K) return;
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
-        const uint32_t v = a.rows[a.beg + a.ne + r].x;
-        X64[(size_t)r * a.Kp + t.k] = warm ? warm[(size_t)t.k * warm_ld + v] : 0.0;
+        const uint32_t slot = a.beg + a.ne + r;
+        const size_t idx = (size_t)r * a.Kp + t.k;
+        double x;
+        if (a.ig_ptr[slot] == a.ig_ptr[slot + 1])
+            x = bS[idx] / dS[idx];
+        else
+            x = warm ? warm[(size_t)t.k * warm_ld + a.rows[slot].x] : 0.0;
+        X64[idx] = x;
     }
 }
 
-// ---- dense Gauss-Jordan per (SCC, system) ---------------------------------------------------
-// One CTA per (SCC j of the group, system k0 + blockIdx.y).  Row a is the equation of the
-// SCC's a-th state: q_a z_a - sum over in-SCC predecessors b of rate(b -> a) z_b = rhs_a.
-__global__ void __launch_bounds__(256) k_sw_dense(SwArgs a, const uint32_t* __restrict__ scc_off,
-                                                  const uint32_t* __restrict__ scc_slots,
-                                                  const uint32_t* __restrict__ dloc,
-                                                  const uint64_t* __restrict__ scr_off, uint64_t scr_stride,
-                                                  double* __restrict__ scratch, int smem_max,
-                                                  const double* __restrict__ Bv, double* __restrict__ Z, int k0) {
-    extern __shared__ double s_dyn[];
-    const int j = blockIdx.x;
-    const int k = k0 + blockIdx.y;
-    if (k >= a.K) return;
-    const uint32_t off = scc_off[j];
-    const int s = (int)(scc_off[j + 1] - off);
-    const int w = s + 1;
-    double* s_rate = s_dyn;                       // 2n rates of system k
-    double* fac = s_dyn + 2 * a.n;                // s factors
-    double* A = (s <= smem_max) ? fac + s : scratch + (size_t)(k - k0) * scr_stride + scr_off[j];
-    for (int idx = threadIdx.x; idx < 2 * a.n; idx += blockDim.x) s_rate[idx] = a.rateT[(size_t)idx * a.Kp + k];
-    for (int idx = threadIdx.x; idx < s * w; idx += blockDim.x) A[idx] = 0.0;
+// ---- CTA-local refinement for groups of small SCCs ----------------------------------------
+// One CTA per (SCC of >= 2 states, 32 systems): lane = system, warp w takes rows w, w + nw, ...
+// Every warp holds all 32 lanes, so the block-wide sums below give every warp the same
+// per-lane scalars and every decision (convergence, stagnation) is uniform across warps
+// without another barrier.  Vectors are the group's [row][Kp] buffers; a CTA touches only
+// the rows of its SCC, because SCCs of one level share no edge.
+struct SwLocal {
+    const uint32_t* off;     // SCC j: slots[off[j] .. off[j+1]), even-parity slots first
+    const uint32_t* ne;      // SCC j: number of even-parity slots
+    const uint32_t* slots;
+    const double* bS;        // reduced rhs (odd rows of the group)
+    const double* dS64;      // Schur diagonal (odd rows)
+    const float* dS32;       // its FP32 copy (mixed method)
+    double* X64;             // odd-row solution, refined in place
+    double* R64;             // odd rows: FP64 true residual
+    double* W64;             // even rows: FP64 elimination, also the FP64 inner solve's even buffer
+    double *R, *R0, *PH, *V, *SH, *TT, *D;  // odd rows, FP64 inner solve
+    // FP32 inner solve: buffers of its own, because CTAs of one launch may be in FP32 and
+    // FP64 steps at the same time
+    float *fR, *fR0, *fPH, *fV, *fSH, *fTT, *fD;  // odd rows
+    float* fW;                                    // even rows
+    double tol2, accept2;
+    int max_iters, max_refine, mixed;
+    unsigned long long* ratio;  // per system: max over SCCs of final |r|^2 / |b|^2 (bits of a double >= 0)
+    int* fail;                  // per system: 1 once an SCC stays above the acceptance residual
+    int* iters;                 // per system: inner iterations, max over SCCs
+};
+
+struct LocalRows {
+    const uint32_t* ev;  // even slots of the SCC
+    const uint32_t* od;  // odd slots
+    int se, so, warp, nw;
+    uint32_t obase;      // first odd slot of the group
+};
+
+// Sums of two per-lane values over the CTA's warps, double-buffered so that the next
+// call may write while slow warps still read the previous result.
+__device__ __forceinline__ void local_sum2(double* red, int& site, const LocalRows& L, int lane, double v0, double v1,
+                                           double& o0, double& o1) {
+    double* rb = red + (site & 1) * (2 * kSwLocalWarps * 32);
+    site++;
+    rb[L.warp * 32 + lane] = v0;
+    rb[kSwLocalWarps * 32 + L.warp * 32 + lane] = v1;
     __syncthreads();
-    for (int r = threadIdx.x; r < s; r += blockDim.x) {
-        const uint32_t slot = scc_slots[off + r];
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < L.nw; w++) {
+        s0 += rb[w * 32 + lane];
+        s1 += rb[kSwLocalWarps * 32 + w * 32 + lane];
+    }
+    o0 = s0;
+    o1 = s1;
+}
+
+// even rows: W_e = (sum over odd in-SCC predecessors o of rate(o -> e) X_o) / q_e
+template <class TC, class TX, class TW>
+__device__ __forceinline__ void local_elim(const SwArgs& a, const Tile& t, const TC* s, const LocalRows& L,
+                                           const TX* X, TW* W, bool act) {
+    for (int i = L.warp; i < L.se; i += L.nw) {
+        const uint32_t slot = L.ev[i];
         const uint2 row = a.rows[slot];
-        const uint32_t v = row.x;
-        double q = 0.0;
-        uint32_t f = row.y;
-        while (f) {
-            const int i = __ffs(f) - 1;
-            f &= f - 1;
-            q += s_rate[2 * i + ((v >> i) & 1u)];
-        }
-        A[(size_t)r * w + r] = q;
-        for (uint32_t e = a.ig_ptr[slot]; e < a.ig_ptr[slot + 1]; e++) {
-            const uint32_t ent = a.ig_ent[e];
-            const int i = (int)(ent & 31u);
-            A[(size_t)r * w + dloc[ent >> 5]] -= s_rate[2 * i + (((v >> i) & 1u) ^ 1u)];
-        }
-        A[(size_t)r * w + s] = Bv[(size_t)(slot - a.beg) * a.Kp + k];
+        const uint32_t p0 = a.ig_ptr[slot];
+        const TC acc = sw_gather<TC, TX>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, L.obase,
+                                         act, (TC)0);
+        if (act) W[(size_t)(slot - a.beg) * a.Kp + t.k] = (TW)(acc / sw_q(s, row.x, row.y, t));
     }
-    for (int p = 0; p < s; p++) {
-        __syncthreads();
-        const double inv = 1.0 / A[(size_t)p * w + p];
-        for (int r = threadIdx.x; r < s; r += blockDim.x) fac[r] = (r == p) ? 0.0 : A[(size_t)r * w + p] * inv;
-        __syncthreads();
-        const int cols = s - p;  // columns p+1 .. s
-        for (int idx = threadIdx.x; idx < s * cols; idx += blockDim.x) {
-            const int r = idx / cols, c = p + 1 + (idx - r * cols);
-            const double fr = fac[r];
-            if (fr != 0.0) A[(size_t)r * w + c] -= fr * A[(size_t)p * w + c];
+}
+
+// BiCGStab on the SCC's odd-row Schur complement (right preconditioner: its diagonal) for
+// the residual R64 scaled by `scale` (1/|R64|, so that FP32 neither underflows nor
+// overflows); the scaled correction is left in D.  `target` is in scaled units.  Lanes
+// with run == false do not write.
+template <class T>
+__device__ int local_inner(const SwArgs& a, const SwLocal& l, const Tile& t, const T* s, const LocalRows& L,
+                           double* red, int& site, bool run, double scale, double target) {
+    constexpr bool f64 = sizeof(T) == 8;
+    T* R = f64 ? (T*)l.R : (T*)l.fR;
+    T* R0 = f64 ? (T*)l.R0 : (T*)l.fR0;
+    T* PH = f64 ? (T*)l.PH : (T*)l.fPH;
+    T* V = f64 ? (T*)l.V : (T*)l.fV;
+    T* SH = f64 ? (T*)l.SH : (T*)l.fSH;
+    T* TT = f64 ? (T*)l.TT : (T*)l.fTT;
+    T* D = f64 ? (T*)l.D : (T*)l.fD;
+    T* WW = f64 ? (T*)l.W64 : (T*)l.fW;
+    const T* dS = sizeof(T) == 8 ? (const T*)l.dS64 : (const T*)l.dS32;
+    const size_t Kp = a.Kp;
+    if (run) {
+        for (int i = L.warp; i < L.so; i += L.nw) {
+            const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+            const T x = (T)(l.R64[idx] * scale);
+            R[idx] = x;
+            R0[idx] = x;
+            D[idx] = 0;
+            PH[idx] = 0;
+            V[idx] = 0;
         }
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < s; r += blockDim.x)
-        Z[(size_t)scc_slots[off + r] * a.Kp + k] = A[(size_t)r * w + s] / A[(size_t)r * w + r];
+    double rho = 1.0, alpha = 0.0, omega = 1.0, beta = 0.0, best = 1.0, dmy;
+    int its = 0, stall = 0;
+    while (__any_sync(0xffffffffu, run)) {
+        if (run) {
+            const T b = (T)beta, w = (T)omega;
+            for (int i = L.warp; i < L.so; i += L.nw) {
+                const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+                const T d = dS[idx];
+                PH[idx] = (R[idx] + b * (d * PH[idx] - w * V[idx])) / d;
+            }
+        }
+        __syncthreads();
+        local_elim<T, T, T>(a, t, s, L, PH, WW, run);
+        __syncthreads();
+        double r0v = 0.0;
+        for (int i = L.warp; i < L.so; i += L.nw) {
+            const uint32_t slot = L.od[i];
+            const uint2 row = a.rows[slot];
+            const uint32_t p0 = a.ig_ptr[slot];
+            const T flow = sw_gather<T, T>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
+                                           run, (T)0);
+            if (run) {
+                const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
+                const T y = sw_q(s, row.x, row.y, t) * PH[idx] - flow;
+                V[idx] = y;
+                r0v += (double)R0[idx] * (double)y;
+            }
+        }
+        local_sum2(red, site, L, t.lane, r0v, 0.0, r0v, dmy);
+        alpha = r0v != 0.0 ? rho / r0v : 0.0;
+        if (run) {
+            const T al = (T)alpha;
+            for (int i = L.warp; i < L.so; i += L.nw) {
+                const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+                SH[idx] = (R[idx] - al * V[idx]) / dS[idx];
+            }
+        }
+        __syncthreads();
+        local_elim<T, T, T>(a, t, s, L, SH, WW, run);
+        __syncthreads();
+        double ts = 0.0, tt = 0.0;
+        for (int i = L.warp; i < L.so; i += L.nw) {
+            const uint32_t slot = L.od[i];
+            const uint2 row = a.rows[slot];
+            const uint32_t p0 = a.ig_ptr[slot];
+            const T flow = sw_gather<T, T>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
+                                           run, (T)0);
+            if (run) {
+                const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
+                const T sh = SH[idx];
+                const T y = sw_q(s, row.x, row.y, t) * sh - flow;
+                TT[idx] = y;
+                ts += (double)y * ((double)dS[idx] * (double)sh);
+                tt += (double)y * (double)y;
+            }
+        }
+        local_sum2(red, site, L, t.lane, ts, tt, ts, tt);
+        omega = tt > 0.0 ? ts / tt : 0.0;
+        double rr = 0.0, rn = 0.0;
+        if (run) {
+            const T al = (T)alpha, w = (T)omega;
+            for (int i = L.warp; i < L.so; i += L.nw) {
+                const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+                const T sh = SH[idx];
+                D[idx] += al * PH[idx] + w * sh;
+                const T rv = dS[idx] * sh - w * TT[idx];
+                R[idx] = rv;
+                rr += (double)rv * (double)rv;
+                rn += (double)R0[idx] * (double)rv;
+            }
+        }
+        local_sum2(red, site, L, t.lane, rr, rn, rr, rn);
+        if (run) {
+            its++;
+            if (rr < 0.5 * best) {
+                best = rr;
+                stall = 0;
+            } else {
+                stall++;
+            }
+            const bool stop = !(rr > target) || its >= l.max_iters || r0v == 0.0 || omega == 0.0 || rn == 0.0 ||
+                              !isfinite(rr) || !isfinite(alpha) || stall >= kSwStall;
+            if (stop) {
+                run = false;
+            } else {
+                beta = (rn / rho) * (alpha / omega);
+                rho = rn;
+            }
+        }
+    }
+    return its;
+}
+
+__global__ void __launch_bounds__(kSwLocalWarps * 32) k_sw_local(SwArgs a, SwLocal l) {
+    extern __shared__ unsigned char s_raw[];
+    double* s64 = reinterpret_cast<double*>(s_raw);
+    float* s32 = reinterpret_cast<float*>(s64 + 2 * a.n * 32);
+    __shared__ double red[2 * 2 * kSwLocalWarps * 32];
+    Tile t;
+    t.KT = 32;
+    t.lane = threadIdx.x & 31;
+    t.rsub = threadIdx.x >> 5;
+    t.RB = blockDim.x >> 5;
+    t.k = blockIdx.y * 32 + t.lane;
+    for (int idx = threadIdx.x; idx < 2 * a.n * 32; idx += blockDim.x) {
+        const double r = a.rateT[(size_t)(idx >> 5) * a.Kp + blockIdx.y * 32 + (idx & 31)];
+        s64[idx] = r;
+        s32[idx] = (float)r;
+    }
+    __syncthreads();
+    const uint32_t off = l.off[blockIdx.x];
+    LocalRows L;
+    L.se = (int)l.ne[blockIdx.x];
+    L.so = (int)(l.off[blockIdx.x + 1] - off) - L.se;
+    L.ev = l.slots + off;
+    L.od = L.ev + L.se;
+    L.warp = t.rsub;
+    L.nw = t.RB;
+    L.obase = a.beg + a.ne;
+    const bool act = t.k < a.K;
+    const size_t Kp = a.Kp;
+    int site = 0;
+    double b2 = 0.0, dmy;
+    if (act) {
+        for (int i = L.warp; i < L.so; i += L.nw) {
+            const double b = l.bS[(size_t)(L.od[i] - L.obase) * Kp + t.k];
+            b2 += b * b;
+        }
+    }
+    local_sum2(red, site, L, t.lane, b2, 0.0, b2, dmy);
+    // Refinement.  The mixed method takes FP32 inner steps first; a system whose FP32 step
+    // raised the true residual has that step undone, and a system whose FP32 steps stop
+    // cutting the residual by 4x (or after three of them) continues with FP64 steps.
+    // Inner solves of one kind run together: the other systems wait for that step.
+    bool done = !act || !(b2 > 0.0), failed = false, use64 = !l.mixed, stepped = false, last32 = false;
+    double prev = 0.0, rr = 0.0, last_nrm = 0.0;
+    int noimp = 0, its = 0, n32 = 0;
+    for (int outer = 0;; outer++) {
+        // true residual R64 = bS - S X64, in FP64
+        local_elim<double, double, double>(a, t, s64, L, l.X64, l.W64, act);
+        __syncthreads();
+        double r2 = 0.0;
+        for (int i = L.warp; i < L.so; i += L.nw) {
+            const uint32_t slot = L.od[i];
+            const uint2 row = a.rows[slot];
+            const uint32_t p0 = a.ig_ptr[slot];
+            const double flow = sw_gather<double, double>(s64, t, a.Kp, row.x, a.ig_ent, p0,
+                                                          (int)(a.ig_ptr[slot + 1] - p0), l.W64, a.beg, act, 0.0);
+            if (act) {
+                const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
+                const double res = l.bS[idx] - (sw_q(s64, row.x, row.y, t) * l.X64[idx] - flow);
+                l.R64[idx] = res;
+                r2 += res * res;
+            }
+        }
+        local_sum2(red, site, L, t.lane, r2, 0.0, rr, dmy);
+        bool revert = false;
+        if (!done) {
+            if (rr <= l.tol2 * b2) {
+                done = true;
+            } else if (stepped && last32 && !(rr < prev)) {
+                revert = true;
+            } else {
+                if (stepped && last32 && !(rr < 0.25 * prev)) use64 = true;
+                if (stepped && !last32 && !(rr < 0.25 * prev)) noimp++;
+                if (noimp >= 2 || outer >= l.max_refine + 3 || !isfinite(rr)) {
+                    done = true;
+                    failed = !(rr <= l.accept2 * b2);
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, revert)) {
+            if (revert) {
+                for (int i = L.warp; i < L.so; i += L.nw) {
+                    const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+                    l.X64[idx] -= last_nrm * (double)l.fD[idx];
+                }
+                use64 = true;
+            }
+            stepped = false;
+            __syncthreads();
+            continue;  // the residual of the restored iterate
+        }
+        if (!__any_sync(0xffffffffu, !done)) break;
+        prev = rr;
+        const bool want32 = !done && !use64;
+        const bool phase32 = __any_sync(0xffffffffu, want32);
+        const bool run = phase32 ? want32 : !done;
+        const double nrm = sqrt(rr), scale = nrm > 0.0 ? 1.0 / nrm : 0.0;
+        const double target = fmax(phase32 ? 1e-10 : 1e-26, 0.01 * l.tol2 * b2 * scale * scale);
+        if (phase32)
+            its += local_inner<float>(a, l, t, s32, L, red, site, run, scale, target);
+        else
+            its += local_inner<double>(a, l, t, s64, L, red, site, run, scale, target);
+        if (run) {
+            for (int i = L.warp; i < L.so; i += L.nw) {
+                const size_t idx = (size_t)(L.od[i] - L.obase) * Kp + t.k;
+                l.X64[idx] += nrm * (phase32 ? (double)l.fD[idx] : l.D[idx]);
+            }
+        }
+        stepped = run;
+        last32 = phase32;
+        last_nrm = nrm;
+        if (run && phase32 && ++n32 >= 3) use64 = true;
+        __syncthreads();
+    }
+    if (act && L.warp == 0) {
+        atomicMax(l.ratio + t.k, (unsigned long long)__double_as_longlong(b2 > 0.0 ? rr / b2 : 0.0));
+        if (failed) l.fail[t.k] = 1;
+        atomicMax(l.iters + t.k, its);
+    }
 }
 
 // ---- terminal masses ----------------------------------------------------------------------
@@ -560,7 +855,7 @@ __global__ void k_sw_rate_table(int n, int K, int Kp, int nrhs, const double* __
 
 // ---- host side ------------------------------------------------------------------------------
 enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R, W_R0, W_PH, W_V, W_SH, W_TT,
-              W_D, W_SCAL, W_ISCAL, W_CNT, W_DENSE, W_COUNT };
+              W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_F0, W_COUNT = W_F0 + 8 };
 
 int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     if (net->sweep) {
@@ -588,8 +883,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     std::vector<uint32_t> slot_of(N, 0xFFFFFFFFu);
     std::vector<uint2> rows;
     rows.reserve(M);
-    std::vector<uint32_t> dscc_off{0}, dscc_slots, dloc(M, 0);
-    std::vector<uint64_t> dscc_scr;
+    std::vector<uint32_t> lsc_off{0}, lsc_ne, lsc_slots;
     for (int c = T; c < n_sccs;) {
         int c1 = c, mx = 0;
         while (c1 < n_sccs && levels[c1] == levels[c]) {
@@ -599,7 +893,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
         SwGroup g{};
         g.beg = (uint32_t)rows.size();
         g.max_scc = mx;
-        g.kind = mx == 1 ? 0 : (mx <= kSwDenseMax ? 1 : 2);
+        g.kind = mx == 1 ? 0 : (mx <= kSwLocalMax ? 1 : 2);
         for (int par = 0; par < 2; par++) {
             for (int p = offsets[c]; p < offsets[c1]; p++) {
                 const uint32_t v = (uint32_t)order[p];
@@ -610,26 +904,32 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
             (par ? g.no : g.ne) = (uint32_t)rows.size() - g.beg - (par ? g.ne : 0);
         }
         if (g.kind == 1) {
-            g.scc0 = (uint32_t)dscc_off.size() - 1;
-            uint64_t scr = 0;
+            // SCCs of >= 2 states, each with its even-parity slots first
+            g.scc0 = (uint32_t)lsc_ne.size();
             for (int cc = c; cc < c1; cc++) {
                 const int sz = offsets[cc + 1] - offsets[cc];
-                for (int p = offsets[cc]; p < offsets[cc + 1]; p++) {
-                    const uint32_t sl = slot_of[(uint32_t)order[p]];
-                    dloc[sl] = (uint32_t)(p - offsets[cc]);
-                    dscc_slots.push_back(sl);
-                }
-                dscc_off.push_back((uint32_t)dscc_slots.size());
-                dscc_scr.push_back(scr);
-                if (sz > kSwDenseSmem) scr += (uint64_t)sz * (sz + 1);
-                g.smax = std::max(g.smax, sz);
+                if (sz < 2) continue;
+                uint32_t ne = 0;
+                for (int par = 0; par < 2; par++)
+                    for (int p = offsets[cc]; p < offsets[cc + 1]; p++) {
+                        const uint32_t v = (uint32_t)order[p];
+                        if ((uint32_t)(__builtin_popcount(v) & 1) != (uint32_t)par) continue;
+                        lsc_slots.push_back(slot_of[v]);
+                        ne += par == 0;
+                    }
+                lsc_off.push_back((uint32_t)lsc_slots.size());
+                lsc_ne.push_back(ne);
+                g.max_odd = std::max(g.max_odd, sz - (int)ne);
             }
-            g.nscc = (uint32_t)(c1 - c);
-            g.scr = scr;
+            g.nscc = (uint32_t)lsc_ne.size() - g.scc0;
         }
         P->max_rows = std::max(P->max_rows, g.ne + g.no);
         P->max_even = std::max(P->max_even, g.ne);
         P->max_odd = std::max(P->max_odd, g.no);
+        if (g.kind == 1) {
+            P->max_even_local = std::max(P->max_even_local, g.ne);
+            P->max_odd_local = std::max(P->max_odd_local, g.no);
+        }
         P->groups.push_back(g);
         c = c1;
     }
@@ -684,14 +984,9 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     up32(P->og_ent, og);
     up32(P->tp_ptr, tp_ptr);
     up32(P->tp_ent, tp);
-    up32(P->dscc_off, dscc_off);
-    up32(P->dscc_slots, dscc_slots);
-    up32(P->dloc, dloc);
-    if (rc == ESL_OK) rc = P->dscc_scr.alloc(dscc_scr.size());
-    if (rc == ESL_OK && !dscc_scr.empty() &&
-        cudaMemcpyAsync(P->dscc_scr.get(), dscc_scr.data(), dscc_scr.size() * 8, cudaMemcpyHostToDevice, s) !=
-            cudaSuccess)
-        rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
+    up32(P->lsc_off, lsc_off);
+    up32(P->lsc_ne, lsc_ne);
+    up32(P->lsc_slots, lsc_slots);
     if (rc == ESL_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
     if (rc != ESL_OK) {
         delete P;
@@ -759,7 +1054,12 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
     double* scal = (double*)ws.get(W_SCAL, (size_t)C_NSCAL * Kp * 8, &st_);
     int* iscal = (int*)ws.get(W_ISCAL, (size_t)I_NISCAL * Kp * 4, &st_);
     int* d_cnt = (int*)ws.get(W_CNT, 64, &st_);
+    // per-system results of the CTA-local groups: max |r|^2/|b|^2, failure flag, iterations
+    unsigned long long* loc_ratio = (unsigned long long*)ws.get(W_LOC, (size_t)Kp * 16, &st_);
     if (st_ != ESL_OK) return st_;
+    int* loc_fail = reinterpret_cast<int*>(loc_ratio + Kp);
+    int* loc_iters = loc_fail + Kp;
+    ESL_CUDA(cudaMemsetAsync(loc_ratio, 0, (size_t)Kp * 16, s));
     SwScalPtr sc;
     for (int j = 0; j < C_NSCAL; j++) sc.c[j] = scal + (size_t)j * Kp;
     for (int j = 0; j < I_NISCAL; j++) sc.i[j] = iscal + (size_t)j * Kp;
@@ -767,8 +1067,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
     k_sw_rate_table<<<dim3((Kp + 127) / 128, 2 * n), 128, 0, s>>>(n, K, Kp, nrhs, rates, rateT);
     ESL_CUDA(cudaGetLastError());
 
-    const int KT64 = tile_for(Kp, n, 8), KT32 = tile_for(Kp, n, 4);
-    const size_t sm64 = (size_t)2 * n * KT64 * 8, sm32 = (size_t)2 * n * KT32 * 4;
+    const int KT64 = tile_for(Kp, n, 8);
+    const size_t sm64 = (size_t)2 * n * KT64 * 8;
     SwArgs a{};
     a.n = n;
     a.K = K;
@@ -807,36 +1107,19 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_rhs<false><<<row_grid(rows, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
             a, P->og_ptr.get(), P->og_ent.get(), x0, x0_ld, Z, Bv);
         ESL_CUDA(cudaGetLastError());
-        if (g.kind == 1) {
-            // dense Gauss-Jordan, systems in chunks that bound the global scratch to ~2 GB
-            st.dense_groups++;
-            int chunk = K;
-            if (g.scr > 0) chunk = (int)std::max<uint64_t>(1, std::min<uint64_t>(K, (256ull << 20) / g.scr));
-            double* scr = g.scr > 0 ? (double*)ws.get(W_DENSE, (size_t)chunk * g.scr * 8, &st_) : nullptr;
-            if (st_ != ESL_OK) return st_;
-            // rates, one factor per row of the largest SCC, and the largest in-smem matrix
-            const int sm_s = std::min(g.smax, kSwDenseSmem);
-            const size_t smem = (size_t)(2 * n + g.smax + (size_t)sm_s * (sm_s + 1)) * 8;
-            ESL_CUDA(cudaFuncSetAttribute(k_sw_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            for (int k0 = 0; k0 < K; k0 += chunk) {
-                const int kc = std::min(chunk, K - k0);
-                ESL_COUNT_LAUNCH();
-                k_sw_dense<<<dim3(g.nscc, kc), 256, smem, s>>>(a, P->dscc_off.get() + g.scc0, P->dscc_slots.get(),
-                                                               P->dloc.get(), P->dscc_scr.get() + g.scc0, g.scr, scr,
-                                                               kSwDenseSmem, Bv, Z, k0);
-                ESL_CUDA(cudaGetLastError());
-            }
-            continue;
-        }
-        // ---- Krylov group ----
-        st.krylov_groups++;
+        // ---- Krylov group (CTA-local or grid-wide) ----
+        if (g.kind == 1)
+            st.local_groups++;
+        else
+            st.krylov_groups++;
         const size_t vo = (size_t)std::max<uint32_t>(P->max_odd, 1) * Kp, ve = (size_t)std::max<uint32_t>(P->max_even, 1) * Kp;
         double* bS = (double*)ws.get(W_BS, vo * 8, &st_);
         double* R64 = (double*)ws.get(W_R64, vo * 8, &st_);
         double* dS64 = (double*)ws.get(W_DS64, vo * 8, &st_);
         float* dS32 = mixed ? (float*)ws.get(W_DS32, vo * 4, &st_) : nullptr;
         double* W64 = (double*)ws.get(W_W64, ve * 8, &st_);
-        const size_t es = mixed ? 4 : 8;
+        // 8 bytes per entry: a mixed solve may continue with FP64 inner steps in these buffers
+        const size_t es = 8;
         void* WT = mixed ? ws.get(W_WT, ve * es, &st_) : (void*)W64;
         void* vR = ws.get(W_R, vo * es, &st_);
         void* vR0 = ws.get(W_R0, vo * es, &st_);
@@ -863,8 +1146,74 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_apply<0, double><<<go, kSwT, gsm64, s>>>(a, nullptr, W64, Bv + (size_t)g.ne * Kp, nullptr, bS,
                                                      sc.c[C_BB], nullptr);
         ESL_COUNT_LAUNCH();
-        k_sw_warm<<<go, kSwT, 0, s>>>(a, o.d_warm, (size_t)net->N, X64);
+        k_sw_init<<<go, kSwT, 0, s>>>(a, o.d_warm, (size_t)net->N, bS, dS64, X64);
         ESL_CUDA(cudaGetLastError());
+        if (g.kind == 1) {
+            SwLocal l{};
+            l.off = P->lsc_off.get() + g.scc0;
+            l.ne = P->lsc_ne.get() + g.scc0;
+            l.slots = P->lsc_slots.get();
+            l.bS = bS;
+            l.dS64 = dS64;
+            l.dS32 = dS32;
+            l.X64 = X64;
+            l.R64 = R64;
+            l.W64 = W64;
+            l.R = (double*)vR;
+            l.R0 = (double*)vR0;
+            l.PH = (double*)vPH;
+            l.V = (double*)vV;
+            l.SH = (double*)vSH;
+            l.TT = (double*)vTT;
+            l.D = (double*)vD;
+            if (mixed) {
+                const size_t lo = (size_t)std::max<uint32_t>(P->max_odd_local, 1) * Kp;
+                const size_t le = (size_t)std::max<uint32_t>(P->max_even_local, 1) * Kp;
+                float** fv[7] = {&l.fR, &l.fR0, &l.fPH, &l.fV, &l.fSH, &l.fTT, &l.fD};
+                for (int j = 0; j < 7; j++) *fv[j] = (float*)ws.get(W_F0 + j, lo * 4, &st_);
+                l.fW = (float*)ws.get(W_F0 + 7, le * 4, &st_);
+                if (st_ != ESL_OK) return st_;
+            }
+            l.tol2 = tol * tol;
+            l.accept2 = kSwAcceptRel * kSwAcceptRel;
+            l.max_iters = max_iters;
+            l.max_refine = max_refine;
+            l.mixed = mixed ? 1 : 0;
+            l.ratio = loc_ratio;
+            l.fail = loc_fail;
+            l.iters = loc_iters;
+            const int nw = std::max(1, std::min(kSwLocalWarps, (g.max_odd + 3) / 4));
+            const size_t smem = (size_t)2 * n * 32 * (8 + 4);
+            if (g.nscc > 0) {
+                ESL_COUNT_LAUNCH();
+                k_sw_local<<<dim3(g.nscc, Kp / 32), nw * 32, smem, s>>>(a, l);
+            }
+            // even rows of the group from the odd solution, straight into Z
+            a.flags = nullptr;
+            a.KT = gKT64;
+            ESL_COUNT_LAUNCH();
+            k_sw_elim<double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
+            ESL_CUDA(cudaGetLastError());
+            if (debug_on()) {
+                std::vector<unsigned long long> h_loc((size_t)Kp * 2);
+                ESL_CUDA(cudaMemcpyAsync(h_loc.data(), loc_ratio, (size_t)Kp * 16, cudaMemcpyDeviceToHost, s));
+                ESL_CUDA(cudaStreamSynchronize(s));
+                const int* h_fail = reinterpret_cast<const int*>(h_loc.data() + Kp);
+                int nf = 0;
+                double worst = 0.0;
+                for (int k = 0; k < K; k++) {
+                    double ratio;
+                    memcpy(&ratio, &h_loc[k], 8);
+                    worst = std::max(worst, ratio);
+                    nf += h_fail[k] != 0;
+                }
+                fprintf(stderr,
+                        "[esl-sweep] local group beg %u even %u odd %u max_scc %d sccs %u warps %d: failed %d "
+                        "worst relres so far %.3e\n",
+                        g.beg, g.ne, g.no, g.max_scc, g.nscc, nw, nf, std::sqrt(worst));
+            }
+            continue;
+        }
         auto true_residual = [&]() -> int {
             a.flags = nullptr;
             a.KT = gKT64;
@@ -904,7 +1253,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 TT* WW = (TT*)(sizeof(TT) == 8 ? (void*)W64 : WT);
                 const TT* dS = (const TT*)(sizeof(TT) == 8 ? (void*)dS64 : (void*)dS32);
                 ESL_COUNT_LAUNCH();
-                k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, R64, R, R0, D, PH, V);
+                k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, R, R0, D, PH, V);
                 int it = 0, chunk = 0;
                 for (; it < max_iters; it += kSwPoll, chunk++) {
                     for (int j = 0; j < kSwPoll; j++) {
@@ -939,7 +1288,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 }
                 group_iters += it;
                 ESL_COUNT_LAUNCH();
-                k_sw_commit<TT><<<goi, kSwT, 0, s>>>(a, D, X64);
+                k_sw_commit<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], D, X64);
                 ESL_CUDA(cudaGetLastError());
                 return ESL_OK;
             };
@@ -983,6 +1332,23 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_term<<<row_grid((uint32_t)P->TS, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
             a, P->TS, net->order.get(), net->term_of.get(), P->tp_ptr.get(), P->tp_ent.get(), x0, x0_ld, Z, T, y);
         ESL_CUDA(cudaGetLastError());
+    }
+    // results of the CTA-local groups
+    if (st.local_groups > 0) {
+        std::vector<unsigned long long> h_loc((size_t)Kp * 2);
+        ESL_CUDA(cudaMemcpyAsync(h_loc.data(), loc_ratio, (size_t)Kp * 16, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        const int* h_fail = reinterpret_cast<const int*>(h_loc.data() + Kp);
+        const int* h_its = h_fail + Kp;
+        int loc_its = 0;
+        for (int k = 0; k < K; k++) {
+            double ratio;
+            memcpy(&ratio, &h_loc[k], 8);
+            st.relres = std::max(st.relres, std::sqrt(ratio));
+            if (h_fail[k]) failed[k] = 1;
+            loc_its = std::max(loc_its, h_its[k]);
+        }
+        total_iters += loc_its;
     }
     st.iters = total_iters;
     st.failed.clear();
