@@ -71,7 +71,7 @@ struct SweepPlan {
     int TS = 0;
     std::vector<SwGroup> groups;
     DevBuf<uint2> rows;                  // per slot: (state, out-mask)
-    DevBuf<uint32_t> ig_ptr, ig_ent;     // predecessors inside the group: slot << 5 | bit
+    DevBuf<uint32_t> ig_ptr, ig_ent;     // predecessors inside the group: slot << 6 | rate index
     DevBuf<uint32_t> og_ptr, og_ent;     // predecessors in earlier groups
     DevBuf<uint32_t> tp_ptr, tp_ent;     // transient predecessors of terminal position p
     DevBuf<uint32_t> lsc_off;            // local SCCs: offsets into lsc_slots
@@ -91,16 +91,21 @@ struct SwArgs {
     const int* flags;        // per-system flags or null
 };
 
+// A tile is KT systems of one row handled by TR = KT / S threads, S systems per thread:
+// thread `lane` of the row owns systems k, k + TR, ..., k + (S - 1) TR.  TR >= 32, so the
+// 32 lanes of a warp always share one row.
 struct Tile {
-    int lane, rsub, RB, KT, k;
+    int lane, rsub, RB, KT, TR, k;
 };
 
+template <int S = 1>
 __device__ __forceinline__ Tile tile_of(int KT) {
     Tile t;
     t.KT = KT;
-    t.RB = blockDim.x / KT;
-    t.lane = threadIdx.x % KT;
-    t.rsub = threadIdx.x / KT;
+    t.TR = KT / S;
+    t.RB = blockDim.x / t.TR;
+    t.lane = threadIdx.x % t.TR;
+    t.rsub = threadIdx.x / t.TR;
     t.k = blockIdx.y * KT + t.lane;
     return t;
 }
@@ -116,23 +121,33 @@ __device__ __forceinline__ void sw_rates(T* s, const SwArgs& a, const Tile& t) {
     __syncthreads();
 }
 
-// out-rate of state v (out-mask f) for this thread's system
-template <class T>
-__device__ __forceinline__ T sw_q(const T* s, uint32_t v, uint32_t f, const Tile& t) {
-    T q = 0;
+// out-rates of state v (out-mask f) for this thread's S systems
+template <int S, class T>
+__device__ __forceinline__ void sw_qs(const T* s, uint32_t v, uint32_t f, const Tile& t, T (&q)[S]) {
+#pragma unroll
+    for (int j = 0; j < S; j++) q[j] = 0;
     while (f) {
         const int i = __ffs(f) - 1;
         f &= f - 1;
-        q += s[(2 * i + ((v >> i) & 1u)) * t.KT + t.lane];
+        const T* r = s + (2 * i + ((v >> i) & 1u)) * t.KT + t.lane;
+#pragma unroll
+        for (int j = 0; j < S; j++) q[j] += r[j * t.TR];
     }
-    return q;
 }
 
-// rate of the edge into v that flips bit i (its source has bit i of v complemented)
 template <class T>
-__device__ __forceinline__ T sw_in(const T* s, uint32_t v, int i, const Tile& t) {
-    return s[(2 * i + (((v >> i) & 1u) ^ 1u)) * t.KT + t.lane];
+__device__ __forceinline__ T sw_q(const T* s, uint32_t v, uint32_t f, const Tile& t) {
+    T q[1];
+    sw_qs<1>(s, v, f, t, q);
+    return q[0];
 }
+
+// Predecessor entries are (slot << 6) | rate index, the rate index of the edge being
+// 2i + b for a flip of bit i out of a source whose bit i is b (rates are
+// [up_0, down_0, up_1, ...]).
+constexpr int kEntShift = 6;
+__device__ __forceinline__ uint32_t ent_slot(uint32_t e) { return e >> kEntShift; }
+__device__ __forceinline__ int ent_rate(uint32_t e) { return (int)(e & 63u); }
 
 __device__ __forceinline__ bool sw_skip(const SwArgs& a, int k) {
     if (k >= a.K) return true;
@@ -141,52 +156,79 @@ __device__ __forceinline__ bool sw_skip(const SwArgs& a, int k) {
     return !(f & SW_RUN) || (f & SW_IDONE);
 }
 
-// Sum over the predecessor entries ent[p0 .. p0 + cnt) of a row with state v of
-// rate(edge into v) * X[(entry >> 5) - base][k], added to acc in entry order.  All 32
-// lanes of a warp handle the same row (tiles are at least 32 systems wide), so the row's
-// entries (at most n <= 27) arrive in one coalesced load and are broadcast by shuffles,
-// and the gathers are issued four at a time.  Every lane of the warp must call it; lanes
-// with act == false load nothing.
-template <class TC, class TX>
-__device__ __forceinline__ TC sw_gather(const TC* s, const Tile& t, int Kp, uint32_t v,
-                                        const uint32_t* __restrict__ ent, uint32_t p0, int cnt,
-                                        const TX* __restrict__ X, uint32_t base, bool act, TC acc) {
+// acc[j] += sum over the predecessor entries ent[p0 .. p0 + cnt) of a row of
+// rate(entry) * X[ent_slot(entry) - base][system j], in entry order.  All 32 lanes of a
+// warp handle the same row, so the row's entries (at most n <= 26) arrive in one
+// coalesced load and are broadcast by shuffles, and the gathers are issued four entries
+// at a time.  Every lane of the warp must call it; systems with act[j] == false load
+// nothing.
+template <int S, class TC, class TX>
+__device__ __forceinline__ void sw_gathers(const TC* s, const Tile& t, int Kp, const uint32_t* __restrict__ ent,
+                                           uint32_t p0, int cnt, const TX* __restrict__ X, uint32_t base,
+                                           const bool (&act)[S], TC (&acc)[S]) {
     const int lane = threadIdx.x & 31;
     const uint32_t mine = lane < cnt ? __ldg(ent + p0 + lane) : 0u;
+    const TX* Xk = X + t.k;
+    const TC* sk = s + t.lane;
     int j = 0;
     for (; j + 4 <= cnt; j += 4) {
         uint32_t e[4];
-        TC x[4];
+        TC x[4][S];
 #pragma unroll
         for (int u = 0; u < 4; u++) e[u] = __shfl_sync(0xffffffffu, mine, j + u);
 #pragma unroll
-        for (int u = 0; u < 4; u++) x[u] = act ? (TC)X[(size_t)((e[u] >> 5) - base) * Kp + t.k] : (TC)0;
+        for (int u = 0; u < 4; u++) {
+            const TX* row = Xk + (size_t)(ent_slot(e[u]) - base) * Kp;
 #pragma unroll
-        for (int u = 0; u < 4; u++) acc += sw_in(s, v, (int)(e[u] & 31u), t) * x[u];
+            for (int q = 0; q < S; q++) x[u][q] = act[q] ? (TC)row[q * t.TR] : (TC)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const TC* r = sk + ent_rate(e[u]) * t.KT;
+#pragma unroll
+            for (int q = 0; q < S; q++) acc[q] += r[q * t.TR] * x[u][q];
+        }
     }
     for (; j < cnt; j++) {
         const uint32_t e = __shfl_sync(0xffffffffu, mine, j);
-        const TC x = act ? (TC)X[(size_t)((e >> 5) - base) * Kp + t.k] : (TC)0;
-        acc += sw_in(s, v, (int)(e & 31u), t) * x;
+        const TX* row = Xk + (size_t)(ent_slot(e) - base) * Kp;
+        const TC* r = sk + ent_rate(e) * t.KT;
+#pragma unroll
+        for (int q = 0; q < S; q++) acc[q] += r[q * t.TR] * (act[q] ? (TC)row[q * t.TR] : (TC)0);
     }
-    return acc;
 }
 
-// Block-wide sums of NV per-thread values for this thread's system, added atomically to
-// dst[j][k] by the first row-lane.
-template <int NV>
-__device__ __forceinline__ void sw_reduce(const double (&v)[NV], double* const (&dst)[NV], const Tile& t, int K) {
-    __shared__ double red[NV * kSwT];
+template <class TC, class TX>
+__device__ __forceinline__ TC sw_gather(const TC* s, const Tile& t, int Kp, const uint32_t* __restrict__ ent,
+                                        uint32_t p0, int cnt, const TX* __restrict__ X, uint32_t base, bool act,
+                                        TC acc) {
+    const bool a1[1] = {act};
+    TC c1[1] = {acc};
+    sw_gathers<1, TC, TX>(s, t, Kp, ent, p0, cnt, X, base, a1, c1);
+    return c1[0];
+}
+
+// Block-wide sums of NV per-thread values for each of this thread's S systems, added
+// atomically to dst[v][system] by the first row of the CTA.
+template <int NV, int S = 1>
+__device__ __forceinline__ void sw_reduce(const double (&v)[NV][S], double* const (&dst)[NV], const Tile& t, int K) {
+    __shared__ double red[NV * S * kSwT];
 #pragma unroll
-    for (int j = 0; j < NV; j++) red[j * kSwT + threadIdx.x] = v[j];
+    for (int j = 0; j < NV; j++)
+#pragma unroll
+        for (int q = 0; q < S; q++) red[(j * S + q) * kSwT + threadIdx.x] = v[j][q];
     __syncthreads();
-    if (t.rsub == 0 && t.k < K) {
+    if (t.rsub == 0) {
 #pragma unroll
-        for (int j = 0; j < NV; j++) {
-            double acc = 0.0;
-            for (int r = 0; r < t.RB; r++) acc += red[j * kSwT + r * t.KT + t.lane];
-            if (acc != 0.0) atomicAdd(dst[j] + t.k, acc);
-        }
+        for (int j = 0; j < NV; j++)
+#pragma unroll
+            for (int q = 0; q < S; q++) {
+                const int k = t.k + q * t.TR;
+                if (k >= K) continue;
+                double acc = 0.0;
+                for (int r = 0; r < t.RB; r++) acc += red[(j * S + q) * kSwT + r * t.TR + t.lane];
+                if (acc != 0.0) atomicAdd(dst[j] + k, acc);
+            }
     }
 }
 
@@ -209,7 +251,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_rhs(SwArgs a, const uint32_t* __res
         const uint32_t v = row.x;
         const uint32_t p0 = og_ptr[slot];
         double acc = act ? x0[(size_t)(t.k % a.nrhs) * x0_ld + v] : 0.0;
-        acc = sw_gather<double, double>(s_rate, t, a.Kp, v, og_ent, p0, (int)(og_ptr[slot + 1] - p0), Z, 0u, act, acc);
+        acc = sw_gather<double, double>(s_rate, t, a.Kp, og_ent, p0, (int)(og_ptr[slot + 1] - p0), Z, 0u, act, acc);
         if (!act) continue;
         if (DIRECT)
             Z[(size_t)slot * a.Kp + t.k] = acc / sw_q(s_rate, v, row.y, t);
@@ -232,10 +274,11 @@ __global__ void __launch_bounds__(kSwT) k_sw_diag(SwArgs a, double* __restrict__
         double d = sw_q(s_rate, o, row.y, t);
         for (uint32_t e = a.ig_ptr[slot]; e < a.ig_ptr[slot + 1]; e++) {
             const uint32_t ent = a.ig_ent[e];
-            const int i = (int)(ent & 31u);
-            if (!((row.y >> i) & 1u)) continue;  // no edge o -> e
-            const uint2 re = a.rows[ent >> 5];
-            d -= sw_in(s_rate, o, i, t) * sw_in(s_rate, re.x, i, t) / sw_q(s_rate, re.x, re.y, t);
+            const int ri = ent_rate(ent);
+            if (!((row.y >> (ri >> 1)) & 1u)) continue;  // no edge o -> e
+            const uint2 re = a.rows[ent_slot(ent)];
+            // rate(e -> o) is the entry's; rate(o -> e) flips the same bit the other way
+            d -= s_rate[ri * t.KT + t.lane] * s_rate[(ri ^ 1) * t.KT + t.lane] / sw_q(s_rate, re.x, re.y, t);
         }
         dS64[(size_t)r * a.Kp + t.k] = d;
         if (dS32) dS32[(size_t)r * a.Kp + t.k] = (float)d;
@@ -244,26 +287,39 @@ __global__ void __launch_bounds__(kSwT) k_sw_diag(SwArgs a, double* __restrict__
 
 // Even-row elimination: W_e = (C_e + sum over in-group odd predecessors o of
 // rate(o -> e) X_o) / q_e.  C (FP64, even rows of the group buffer) and X may be null.
-template <class TX, class TW, class TC>
+// S systems per thread.
+template <int S, class TX, class TW, class TC>
 __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __restrict__ C, const TX* __restrict__ X,
                                                   TW* __restrict__ W) {
     extern __shared__ unsigned char s_raw[];
     TC* s_rate = reinterpret_cast<TC*>(s_raw);
-    const Tile t = tile_of(a.KT);
+    const Tile t = tile_of<S>(a.KT);
     sw_rates(s_rate, a, t);
-    const bool act = !sw_skip(a, t.k);
-    if (__all_sync(0xffffffffu, !act)) return;
+    bool act[S];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+        act[q] = !sw_skip(a, t.k + q * t.TR);
+        any |= act[q];
+    }
+    if (!__any_sync(0xffffffffu, any)) return;
     const uint32_t obase = a.beg + a.ne;
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne; r += gridDim.x * t.RB) {
         const uint32_t slot = a.beg + r;
         const uint2 row = a.rows[slot];
-        const uint32_t v = row.x;
-        TC acc = (C && act) ? (TC)C[(size_t)r * a.Kp + t.k] : (TC)0;
+        const size_t idx = (size_t)r * a.Kp + t.k;
+        TC acc[S];
+#pragma unroll
+        for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q * t.TR] : (TC)0;
         if (X) {
             const uint32_t p0 = a.ig_ptr[slot];
-            acc = sw_gather<TC, TX>(s_rate, t, a.Kp, v, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, obase, act, acc);
+            sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, obase, act, acc);
         }
-        if (act) W[(size_t)r * a.Kp + t.k] = (TW)(acc / sw_q(s_rate, v, row.y, t));
+        TC qv[S];
+        sw_qs<S>(s_rate, row.x, row.y, t, qv);
+#pragma unroll
+        for (int q = 0; q < S; q++)
+            if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] / qv[q]);
     }
 }
 
@@ -272,56 +328,80 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
 //   MODE 1: Y = B - y                    (true residual, FP64), acc0 += Y^2
 //   MODE 2: Y = y                        acc0 += AUX . Y   (AUX = r0)
 //   MODE 3: Y = y                        acc0 += Y . (AUX X), acc1 += Y . Y   (AUX = dS)
-template <int MODE, class T>
+// S systems per thread.  X, AUX and Y are streamed (evict-first) so that the gathered W
+// keeps its place in L2.
+template <int S, int MODE, class T>
 __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict__ X, const T* __restrict__ W,
                                                    const double* __restrict__ B, const T* __restrict__ AUX,
                                                    T* __restrict__ Y, double* acc0, double* acc1) {
     extern __shared__ unsigned char s_raw[];
     T* s_rate = reinterpret_cast<T*>(s_raw);
-    const Tile t = tile_of(a.KT);
+    const Tile t = tile_of<S>(a.KT);
     sw_rates(s_rate, a, t);
-    double d0 = 0.0, d1 = 0.0;
-    const bool act = !((MODE >= 2) ? sw_skip(a, t.k) : (t.k >= a.K));
-    if (__any_sync(0xffffffffu, act)) {
+    double d0[S], d1[S];
+    bool act[S];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+        d0[q] = d1[q] = 0.0;
+        const int k = t.k + q * t.TR;
+        act[q] = !((MODE >= 2) ? sw_skip(a, k) : (k >= a.K));
+        any |= act[q];
+    }
+    if (__any_sync(0xffffffffu, any)) {
         for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
             const uint32_t slot = a.beg + a.ne + r;
             const uint2 row = a.rows[slot];
-            const uint32_t o = row.x;
             const size_t idx = (size_t)r * a.Kp + t.k;
             const uint32_t p0 = a.ig_ptr[slot];
-            const T flow = sw_gather<T, T>(s_rate, t, a.Kp, o, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), W, a.beg,
-                                           act, (T)0);
-            if (!act) continue;
-            if (MODE == 0) {
-                const double y = B[idx] + (double)flow;
-                Y[idx] = (T)y;
-                d0 += y * y;
-            } else {
-                const T x = X[idx];
-                const T y = sw_q(s_rate, o, row.y, t) * x - flow;
-                if (MODE == 1) {
-                    const double res = B[idx] - (double)y;
-                    Y[idx] = (T)res;
-                    d0 += res * res;
-                } else if (MODE == 2) {
-                    Y[idx] = y;
-                    d0 += (double)AUX[idx] * (double)y;
+            T flow[S];
+#pragma unroll
+            for (int q = 0; q < S; q++) flow[q] = 0;
+            sw_gathers<S, T, T>(s_rate, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), W, a.beg, act, flow);
+            T qv[S];
+            if (MODE != 0) sw_qs<S>(s_rate, row.x, row.y, t, qv);
+#pragma unroll
+            for (int q = 0; q < S; q++) {
+                if (!act[q]) continue;
+                const size_t i = idx + q * t.TR;
+                if (MODE == 0) {
+                    const double y = B[i] + (double)flow[q];
+                    Y[i] = (T)y;
+                    d0[q] += y * y;
                 } else {
-                    Y[idx] = y;
-                    d0 += (double)y * ((double)AUX[idx] * (double)x);
-                    d1 += (double)y * (double)y;
+                    const T x = __ldcs(X + i);
+                    const T y = qv[q] * x - flow[q];
+                    if (MODE == 1) {
+                        const double res = B[i] - (double)y;
+                        Y[i] = (T)res;
+                        d0[q] += res * res;
+                    } else if (MODE == 2) {
+                        __stcs(Y + i, y);
+                        d0[q] += (double)__ldcs(AUX + i) * (double)y;
+                    } else {
+                        __stcs(Y + i, y);
+                        d0[q] += (double)y * ((double)__ldcs(AUX + i) * (double)x);
+                        d1[q] += (double)y * (double)y;
+                    }
                 }
             }
         }
     }
     if (MODE == 3) {
-        double v[2] = {d0, d1};
+        double v[2][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) {
+            v[0][q] = d0[q];
+            v[1][q] = d1[q];
+        }
         double* const dst[2] = {acc0, acc1};
-        sw_reduce<2>(v, dst, t, a.K);
+        sw_reduce<2, S>(v, dst, t, a.K);
     } else {
-        double v[1] = {d0};
+        double v[1][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) v[0][q] = d0[q];
         double* const dst[1] = {acc0};
-        sw_reduce<1>(v, dst, t, a.K);
+        sw_reduce<1, S>(v, dst, t, a.K);
     }
 }
 
@@ -370,15 +450,15 @@ __global__ void __launch_bounds__(kSwT) k_sw_xr(SwArgs a, SwScalPtr sc, const T*
         const T omega = tt > 0.0 ? (T)(sc.c[C_TS][t.k] / tt) : (T)0;
         for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
             const size_t idx = (size_t)r * a.Kp + t.k;
-            const T sh = SH[idx];
-            D[idx] += alpha * PH[idx] + omega * sh;
-            const T rn = dS[idx] * sh - omega * TT[idx];
-            R[idx] = rn;
+            const T sh = __ldcs(SH + idx);
+            __stcs(D + idx, __ldcs(D + idx) + alpha * __ldcs(PH + idx) + omega * sh);
+            const T rn = __ldcs(dS + idx) * sh - omega * __ldcs(TT + idx);
+            __stcs(R + idx, rn);
             d0 += (double)rn * (double)rn;
-            d1 += (double)R0[idx] * (double)rn;
+            d1 += (double)__ldcs(R0 + idx) * (double)rn;
         }
     }
-    double v[2] = {d0, d1};
+    double v[2][1] = {{d0}, {d1}};
     double* const dst[2] = {sc.c[C_RR], sc.c[C_RN]};
     sw_reduce<2>(v, dst, t, a.K);
 }
@@ -573,7 +653,7 @@ __device__ __forceinline__ void local_elim(const SwArgs& a, const Tile& t, const
         const uint32_t slot = L.ev[i];
         const uint2 row = a.rows[slot];
         const uint32_t p0 = a.ig_ptr[slot];
-        const TC acc = sw_gather<TC, TX>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, L.obase,
+        const TC acc = sw_gather<TC, TX>(s, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, L.obase,
                                          act, (TC)0);
         if (act) W[(size_t)(slot - a.beg) * a.Kp + t.k] = (TW)(acc / sw_q(s, row.x, row.y, t));
     }
@@ -628,7 +708,7 @@ __device__ int local_inner(const SwArgs& a, const SwLocal& l, const Tile& t, con
             const uint32_t slot = L.od[i];
             const uint2 row = a.rows[slot];
             const uint32_t p0 = a.ig_ptr[slot];
-            const T flow = sw_gather<T, T>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
+            const T flow = sw_gather<T, T>(s, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
                                            run, (T)0);
             if (run) {
                 const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
@@ -654,7 +734,7 @@ __device__ int local_inner(const SwArgs& a, const SwLocal& l, const Tile& t, con
             const uint32_t slot = L.od[i];
             const uint2 row = a.rows[slot];
             const uint32_t p0 = a.ig_ptr[slot];
-            const T flow = sw_gather<T, T>(s, t, a.Kp, row.x, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
+            const T flow = sw_gather<T, T>(s, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), WW, a.beg,
                                            run, (T)0);
             if (run) {
                 const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
@@ -709,6 +789,7 @@ __global__ void __launch_bounds__(kSwLocalWarps * 32) k_sw_local(SwArgs a, SwLoc
     __shared__ double red[2 * 2 * kSwLocalWarps * 32];
     Tile t;
     t.KT = 32;
+    t.TR = 32;
     t.lane = threadIdx.x & 31;
     t.rsub = threadIdx.x >> 5;
     t.RB = blockDim.x >> 5;
@@ -755,7 +836,7 @@ __global__ void __launch_bounds__(kSwLocalWarps * 32) k_sw_local(SwArgs a, SwLoc
             const uint32_t slot = L.od[i];
             const uint2 row = a.rows[slot];
             const uint32_t p0 = a.ig_ptr[slot];
-            const double flow = sw_gather<double, double>(s64, t, a.Kp, row.x, a.ig_ent, p0,
+            const double flow = sw_gather<double, double>(s64, t, a.Kp, a.ig_ent, p0,
                                                           (int)(a.ig_ptr[slot + 1] - p0), l.W64, a.beg, act, 0.0);
             if (act) {
                 const size_t idx = (size_t)(slot - L.obase) * Kp + t.k;
@@ -839,7 +920,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_term(SwArgs a, int TS, const int32_
         double acc = x0[(size_t)(t.k % a.nrhs) * x0_ld + v];
         for (uint32_t e = tp_ptr[p]; e < tp_ptr[p + 1]; e++) {
             const uint32_t ent = tp_ent[e];
-            acc += sw_in(s_rate, v, (int)(ent & 31u), t) * Z[(size_t)(ent >> 5) * a.Kp + t.k];
+            acc += s_rate[ent_rate(ent) * t.KT + t.lane] * Z[(size_t)ent_slot(ent) * a.Kp + t.k];
         }
         atomicAdd(&y[(size_t)t.k * T + term_of[v]], acc);
     }
@@ -947,7 +1028,9 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
                 in &= in - 1;
                 const uint32_t su = slot_of[v ^ (1u << i)];
                 if (su == 0xFFFFFFFFu) continue;  // a terminal state has no edge out of its SCC
-                ((su >= g.beg && su < end) ? ig : og).push_back((su << 5) | (uint32_t)i);
+                // source bit i is the complement of v's
+                const uint32_t ri = 2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u);
+                ((su >= g.beg && su < end) ? ig : og).push_back((su << 6) | ri);
             }
             ig_ptr.push_back((uint32_t)ig.size());
             og_ptr.push_back((uint32_t)og.size());
@@ -961,7 +1044,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
             const int i = __builtin_ctz(in);
             in &= in - 1;
             const uint32_t su = slot_of[v ^ (1u << i)];
-            if (su != 0xFFFFFFFFu) tp.push_back((su << 5) | (uint32_t)i);
+            if (su != 0xFFFFFFFFu) tp.push_back((su << 6) | (2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u)));
         }
         tp_ptr.push_back((uint32_t)tp.size());
     }
@@ -1001,13 +1084,23 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
 
 // systems per CTA tile: a divisor of Kp, at most 128, and rates of the tile within 40 KB.
 // With `rows` > 0 the tile is also narrowed (down to 32) until one tile's slice of a
-// vector over `rows` rows fits in kSwTileBytes, so that the neighbour gathers of a
-// Krylov iteration hit L2.
-constexpr size_t kSwTileBytes = 48ull << 20;
+// vector over `rows` rows fits in the slice budget, so that the neighbour gathers of a
+// Krylov iteration hit L2.  The budget is a tuning parameter (ESL_SWEEP_TILE_MB,
+// default 48).
+size_t tile_bytes() {
+    static size_t b = 0;
+    if (b == 0) {
+        const char* e = getenv("ESL_SWEEP_TILE_MB");
+        const long mb = e ? atol(e) : 0;
+        b = (size_t)(mb > 0 ? mb : 48) << 20;
+    }
+    return b;
+}
+
 int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0) {
     int kt = 128;
     while (kt > 32 && (Kp % kt != 0 || (size_t)2 * n * kt * elem > 40 * 1024 ||
-                       (size_t)rows * kt * elem > kSwTileBytes))
+                       (size_t)rows * kt * elem > tile_bytes()))
         kt >>= 1;
     return kt;
 }
@@ -1015,8 +1108,8 @@ int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0) {
 // Grid of a row kernel: blockIdx.y is the system tile, blockIdx.x strides over rows.
 // Each tile gets up to 8 CTAs per SM, so a large group fills the GPU with one tile at a
 // time (CTAs are dispatched x-fastest) and its working set stays that tile's slice.
-dim3 row_grid(uint32_t rows, int Kp, int KT, int sm_count) {
-    const int RB = kSwT / KT;
+dim3 row_grid(uint32_t rows, int Kp, int KT, int sm_count, int S = 1) {
+    const int RB = kSwT / (KT / S);
     const unsigned ty = (unsigned)(Kp / KT);
     uint64_t want = ((uint64_t)rows + RB - 1) / RB;
     const uint64_t cap = std::max<uint64_t>(1, (uint64_t)sm_count * 8);
@@ -1035,11 +1128,12 @@ bool debug_on() {
 
 void free_sweep_workspace(void* w) { delete static_cast<Workspace*>(w); }
 
-bool sweep_supported(const esl_net* net) { return net->n >= 1 && net->n <= 27; }
+// slots are packed into 26 bits of a predecessor entry
+bool sweep_supported(const esl_net* net) { return net->n >= 1 && net->n <= 26; }
 
 int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
                   size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st) {
-    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 27 nodes");
+    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
     SweepPlan* P = nullptr;
     ESL_TRY(build_plan(ctx, net, P));
     if (!ctx->sweep_work) ctx->sweep_work = new Workspace();
@@ -1141,9 +1235,9 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_diag<<<go, kSwT, gsm64, s>>>(a, dS64, dS32);
         // reduced rhs bS = b_odd + A_oe (b_even / q_e)
         ESL_COUNT_LAUNCH();
-        k_sw_elim<double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, (const double*)nullptr, W64);
+        k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, (const double*)nullptr, W64);
         ESL_COUNT_LAUNCH();
-        k_sw_apply<0, double><<<go, kSwT, gsm64, s>>>(a, nullptr, W64, Bv + (size_t)g.ne * Kp, nullptr, bS,
+        k_sw_apply<1, 0, double><<<go, kSwT, gsm64, s>>>(a, nullptr, W64, Bv + (size_t)g.ne * Kp, nullptr, bS,
                                                      sc.c[C_BB], nullptr);
         ESL_COUNT_LAUNCH();
         k_sw_init<<<go, kSwT, 0, s>>>(a, o.d_warm, (size_t)net->N, bS, dS64, X64);
@@ -1192,7 +1286,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             a.flags = nullptr;
             a.KT = gKT64;
             ESL_COUNT_LAUNCH();
-            k_sw_elim<double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
+            k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
             ESL_CUDA(cudaGetLastError());
             if (debug_on()) {
                 std::vector<unsigned long long> h_loc((size_t)Kp * 2);
@@ -1219,9 +1313,9 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             a.KT = gKT64;
             ESL_CUDA(cudaMemsetAsync(sc.c[C_RR64], 0, (size_t)Kp * 8, s));
             ESL_COUNT_LAUNCH();
-            k_sw_elim<double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
+            k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
             ESL_COUNT_LAUNCH();
-            k_sw_apply<1, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, R64, sc.c[C_RR64], nullptr);
+            k_sw_apply<1, 1, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, R64, sc.c[C_RR64], nullptr);
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         };
@@ -1241,6 +1335,10 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             a.KT = inner64 ? gKT64 : gKT32;
             const size_t smT = inner64 ? gsm64 : gsm32;
             const dim3 gei = row_grid(g.ne, Kp, a.KT, ctx->sm_count), goi = row_grid(g.no, Kp, a.KT, ctx->sm_count);
+            // two systems per thread in the gather kernels when the tile is wide enough
+            const bool s2 = a.KT >= 64;
+            const dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2),
+                       goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
             auto run_inner = [&](auto tag) -> int {
                 using TT = decltype(tag);
                 TT* R = (TT*)vR;
@@ -1260,15 +1358,29 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                         ESL_COUNT_LAUNCH();
                         k_sw_p<TT><<<goi, kSwT, 0, s>>>(a, sc, R, dS, V, PH);
                         ESL_COUNT_LAUNCH();
-                        k_sw_elim<TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                        if (s2)
+                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                        else
+                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
                         ESL_COUNT_LAUNCH();
-                        k_sw_apply<2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                        if (s2)
+                            k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                        else
+                            k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
                         ESL_COUNT_LAUNCH();
                         k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
                         ESL_COUNT_LAUNCH();
-                        k_sw_elim<TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                        if (s2)
+                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                        else
+                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
                         ESL_COUNT_LAUNCH();
-                        k_sw_apply<3, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS], sc.c[C_TT]);
+                        if (s2)
+                            k_sw_apply<2, 3, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                          sc.c[C_TT]);
+                        else
+                            k_sw_apply<1, 3, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                          sc.c[C_TT]);
                         ESL_COUNT_LAUNCH();
                         k_sw_xr<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, D, R);
                         ESL_COUNT_LAUNCH();
@@ -1305,7 +1417,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         a.flags = nullptr;
         a.KT = gKT64;
         ESL_COUNT_LAUNCH();
-        k_sw_elim<double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
+        k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
         ESL_CUDA(cudaGetLastError());
         h_flags.resize(K);
         std::vector<double> h_rr(K), h_bb(K);
