@@ -221,7 +221,7 @@ def run_ours(args, rank, world, device):
             "e2e": {"value": solves / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "wall_s": e2e_wall},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "schur_operator (k_elim + k_apply)",
+            "roofline": {"bound": "hbm", "kernel": "schur_operator (k_sw_elim + k_sw_apply)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None,
                          "peak_kind": peak_kind,

@@ -64,6 +64,7 @@ struct SwGroup {
     int max_scc;
     uint32_t scc0, nscc;   // local groups: range in the local SCC list (SCCs of >= 2 states)
     int max_odd;           // local groups: most odd rows of one SCC
+    uint64_t nin;          // in-group predecessor entries of the group's rows
 };
 
 struct SweepPlan {
@@ -1018,7 +1019,8 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     std::vector<uint32_t> ig_ptr{0}, og_ptr{0}, ig, og;
     ig_ptr.reserve(M + 1);
     og_ptr.reserve(M + 1);
-    for (const SwGroup& g : P->groups) {
+    for (SwGroup& g : P->groups) {
+        const size_t ig0 = ig.size();
         const uint32_t end = g.beg + g.ne + g.no;
         for (uint32_t sl = g.beg; sl < end; sl++) {
             const uint32_t v = rows[sl].x;
@@ -1035,6 +1037,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
             ig_ptr.push_back((uint32_t)ig.size());
             og_ptr.push_back((uint32_t)og.size());
         }
+        g.nin = ig.size() - ig0;
     }
     std::vector<uint32_t> tp_ptr{0}, tp;
     for (int p = 0; p < TS; p++) {
@@ -1350,6 +1353,11 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 TT* D = (TT*)vD;
                 TT* WW = (TT*)(sizeof(TT) == 8 ? (void*)W64 : WT);
                 const TT* dS = (const TT*)(sizeof(TT) == 8 ? (void*)dS64 : (void*)dS32);
+                // measurement hook: one operator application (k_sw_elim + k_sw_apply) per
+                // iteration of the first poll window, when every started system still runs
+                const int nrun = h_cnt[0];
+                const double op_bytes = (double)nrun * sizeof(TT) * (4.0 * g.no + 2.0 * g.ne) +
+                                        12.0 * (g.ne + g.no) + 4.0 * (double)g.nin;
                 ESL_COUNT_LAUNCH();
                 k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, R, R0, D, PH, V);
                 int it = 0, chunk = 0;
@@ -1357,6 +1365,13 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                     for (int j = 0; j < kSwPoll; j++) {
                         ESL_COUNT_LAUNCH();
                         k_sw_p<TT><<<goi, kSwT, 0, s>>>(a, sc, R, dS, V, PH);
+                        const bool rec = ctx->prof && chunk == 0;
+                        cudaEvent_t ea = nullptr, eb = nullptr;
+                        if (rec) {
+                            ea = ctx->prof_event();
+                            eb = ctx->prof_event();
+                            ESL_CUDA(cudaEventRecord(ea, s));
+                        }
                         ESL_COUNT_LAUNCH();
                         if (s2)
                             k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
@@ -1367,6 +1382,10 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                             k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
                         else
                             k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                        if (rec) {
+                            ESL_CUDA(cudaEventRecord(eb, s));
+                            ctx->prof_recs.push_back({ea, eb, op_bytes});
+                        }
                         ESL_COUNT_LAUNCH();
                         k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
                         ESL_COUNT_LAUNCH();
