@@ -36,6 +36,7 @@ extern "C" {
 typedef struct esl_ctx esl_ctx;     /* device + stream + scratch */
 typedef struct esl_model esl_model; /* parsed bnet: node names + DNF clauses */
 typedef struct esl_net esl_net;     /* device symbolic data for one (model, zero-rate pattern) */
+typedef struct esl_mlp esl_mlp;     /* learned warm start of one network's transient solve */
 
 /* Solver method for the transient absorption and large terminal kernels. */
 #define ESL_METHOD_FP64 0    /* FP64 BiCGStab on the red-black reduced system of all transient states;
@@ -50,6 +51,10 @@ typedef struct esl_solve_opts {
     int max_iters;         /* Krylov iteration budget per system before the fallback (default 600) */
     int max_refine;        /* FP64 refinement steps (default 6) */
     const double* d_warm;  /* optional warm start of the occupation vector, B x N (device), or NULL */
+    double* d_occupation;  /* optional output (device, B x R x N): expected time spent in each transient
+                              state before absorption (0 on terminal states); ESL_METHOD_DIRECT or
+                              ESL_METHOD_MIXED only.  No counterpart in the reference, which never
+                              forms this vector; it is the label the learned warm start trains on. */
 } esl_solve_opts;
 
 typedef struct esl_report {
@@ -159,6 +164,43 @@ int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rat
  * results copied back to host buffers.  Builds and frees its own net. */
 int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,
                    double* x_inf, double* marginals, const esl_solve_opts* opts, esl_report* report);
+
+/* ---- learned warm start.  No counterpart in the reference, which has no learned
+ *      component.  A 3-layer MLP (77 -> 128 -> 128 -> 1, BF16 weights, FP32
+ *      accumulation) predicts the log occupation of a transient state under a rate set
+ *      from: 20 node bits, the log outgoing rate sum, 16 terminal-reachability bits
+ *      and 40 log rates.  Its prediction is the warm start (esl_solve_opts.d_warm) of
+ *      the level sweep's grid-wide Krylov groups; the solve itself is unchanged and
+ *      still decides convergence.  Networks of at most 20 nodes; the handle refers to
+ *      `net`, which must outlive it.  Training labels come from esl_solve_batch with
+ *      esl_solve_opts.d_occupation.  Parameters: W1[128][77], b1[128], W2[128][128],
+ *      b2[128], w3[128], b3 (FP32 master copy). */
+#define ESL_MLP_PARAMS 26625
+int esl_mlp_create(esl_ctx* ctx, const esl_net* net, uint64_t seed, esl_mlp** out);
+int esl_mlp_free(esl_mlp* mlp);
+/* number of states it predicts (odd-parity rows of the grid-wide level groups) and the
+ * label standardisation log z = mu + sigma * y */
+int esl_mlp_info(const esl_mlp* mlp, int* n_targets, float* mu, float* sigma);
+int esl_mlp_targets(const esl_mlp* mlp, uint32_t* d_states);  /* n_targets states */
+int esl_mlp_reach(const esl_mlp* mlp, uint32_t* d_reach);     /* N words: bit t = reaches terminal t */
+int esl_mlp_get_params(const esl_mlp* mlp, float* params);    /* host, ESL_MLP_PARAMS floats */
+int esl_mlp_set_params(esl_mlp* mlp, const float* params, float mu, float sigma);
+/* feature rows (S x 80 floats, device) of samples (rate set d_k[s] of d_rates, state d_state[s]) */
+int esl_mlp_features(esl_mlp* mlp, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
+                     float* d_x);
+/* mean squared error against standardized targets and, if grad != NULL, its gradient
+ * with respect to the parameters (host, ESL_MLP_PARAMS floats) */
+int esl_mlp_loss_grad(esl_mlp* mlp, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
+                      const float* d_target, float* loss, float* grad);
+/* standardized outputs y of the training forward pass (device, S floats) */
+int esl_mlp_forward(esl_mlp* mlp, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
+                    float* d_y);
+/* Adam steps on random (rate set, target state) samples of B rate sets and their
+ * occupations (d_occupation B x N, from esl_solve_batch) */
+int esl_mlp_train(esl_mlp* mlp, int B, const double* d_rates, const double* d_occupation, int steps, int batch,
+                  float lr, float* final_loss);
+/* warm start d_warm (B x N, device) for B rate sets: predicted occupation on the targets, 0 elsewhere */
+int esl_mlp_predict(esl_mlp* mlp, int B, const double* d_rates, double* d_warm);
 
 /* ---- measurement hook (no counterpart in the reference): when on, the solver
  *      records CUDA events around every application of the reduced (Schur) operator

@@ -42,7 +42,7 @@ class EslError(RuntimeError):
 
 class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("tol", C.c_double), ("max_iters", C.c_int), ("max_refine", C.c_int),
-                ("d_warm", C.c_void_p)]
+                ("d_warm", C.c_void_p), ("d_occupation", C.c_void_p)]
 
 
 class Report(C.Structure):
@@ -95,6 +95,19 @@ def lib():
     L.esl_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_batch.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_host.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
+    f32 = C.c_float
+    L.esl_mlp_create.argtypes = [vp, vp, C.c_uint64, P(vp)]
+    L.esl_mlp_free.argtypes = [vp]
+    L.esl_mlp_info.argtypes = [vp, P(C.c_int), P(f32), P(f32)]
+    L.esl_mlp_targets.argtypes = [vp, vp]
+    L.esl_mlp_reach.argtypes = [vp, vp]
+    L.esl_mlp_get_params.argtypes = [vp, vp]
+    L.esl_mlp_set_params.argtypes = [vp, vp, f32, f32]
+    L.esl_mlp_features.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.esl_mlp_loss_grad.argtypes = [vp, C.c_int, vp, vp, vp, vp, P(f32), vp]
+    L.esl_mlp_forward.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.esl_mlp_train.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_int, f32, P(f32)]
+    L.esl_mlp_predict.argtypes = [vp, C.c_int, vp, vp]
     _lib = L
     return L
 
@@ -301,6 +314,117 @@ class Net:
         return bool(ok.value)
 
 
+MLP_PARAMS = 26625
+
+
+class Mlp:
+    """Learned warm start of one network's transient solve (``esl_mlp_*``): a 3-layer
+    MLP (77 -> 128 -> 128 -> 1) predicting the log occupation of the states whose warm
+    start the level sweep's grid-wide Krylov groups read.  Keeps ``net`` alive."""
+
+    def __init__(self, ctx: Context, net: Net, seed: int = 0):
+        self.ctx, self.net = ctx, net
+        h = C.c_void_p()
+        check(lib().esl_mlp_create(ctx._h, net._h, seed, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.esl_mlp_free(self._h)
+            self._h = None
+
+    def info(self):
+        nt, mu, sg = C.c_int(), C.c_float(), C.c_float()
+        check(lib().esl_mlp_info(self._h, C.byref(nt), C.byref(mu), C.byref(sg)))
+        return nt.value, mu.value, sg.value
+
+    @property
+    def n_targets(self) -> int:
+        return self.info()[0]
+
+    def _dev(self):
+        return f"cuda:{self.ctx.device}"
+
+    def targets(self):
+        torch = _torch()
+        t = torch.empty(max(self.n_targets, 1), dtype=torch.int32, device=self._dev())
+        check(lib().esl_mlp_targets(self._h, _ptr(t)))
+        self.ctx.synchronize()
+        return t[: self.n_targets]
+
+    def reach(self):
+        torch = _torch()
+        t = torch.empty(self.net.N, dtype=torch.int32, device=self._dev())
+        check(lib().esl_mlp_reach(self._h, _ptr(t)))
+        self.ctx.synchronize()
+        return t
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(MLP_PARAMS, np.float32)
+        check(lib().esl_mlp_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, params: np.ndarray, mu: float, sigma: float):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == MLP_PARAMS
+        check(lib().esl_mlp_set_params(self._h, _ptr(p), float(mu), float(sigma)))
+
+    def _samples(self, rates, ks, vs):
+        torch = _torch()
+        dev = self._dev()
+        rates = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
+        ks = torch.as_tensor(ks, dtype=torch.int32, device=dev).contiguous()
+        vs = torch.as_tensor(vs, dtype=torch.int32, device=dev).contiguous()
+        return rates, ks, vs
+
+    def features(self, rates, ks, vs):
+        torch = _torch()
+        rates, ks, vs = self._samples(rates, ks, vs)
+        x = torch.empty((ks.numel(), 80), dtype=torch.float32, device=self._dev())
+        check(lib().esl_mlp_features(self._h, ks.numel(), _ptr(rates), _ptr(ks), _ptr(vs), _ptr(x)))
+        self.ctx.synchronize()
+        return x
+
+    def loss_grad(self, rates, ks, vs, targets, grad: bool = True):
+        torch = _torch()
+        rates, ks, vs = self._samples(rates, ks, vs)
+        t = torch.as_tensor(targets, dtype=torch.float32, device=self._dev()).contiguous()
+        loss = C.c_float()
+        g = np.zeros(MLP_PARAMS, np.float32) if grad else None
+        check(lib().esl_mlp_loss_grad(self._h, ks.numel(), _ptr(rates), _ptr(ks), _ptr(vs), _ptr(t),
+                                      C.byref(loss), _ptr(g)))
+        return loss.value, g
+
+    def forward(self, rates, ks, vs):
+        torch = _torch()
+        rates, ks, vs = self._samples(rates, ks, vs)
+        y = torch.empty(ks.numel(), dtype=torch.float32, device=self._dev())
+        check(lib().esl_mlp_forward(self._h, ks.numel(), _ptr(rates), _ptr(ks), _ptr(vs), _ptr(y)))
+        self.ctx.synchronize()
+        return y
+
+    def train(self, rates, occupation, steps: int = 1000, batch: int = 16384, lr: float = 1e-3) -> float:
+        """Adam steps on random (rate set, target state) pairs; ``occupation`` is the
+        B x N output of solve_batch(..., occupation=...) for the B rate sets."""
+        torch = _torch()
+        rates = torch.as_tensor(rates, dtype=torch.float64, device=self._dev()).contiguous()
+        loss = C.c_float()
+        check(lib().esl_mlp_train(self._h, rates.shape[0], _ptr(rates), _ptr(occupation), steps, batch, lr,
+                                  C.byref(loss)))
+        return loss.value
+
+    def predict(self, rates, out=None):
+        """Warm start (B x N, float64, device): predicted occupation on the targets, 0 elsewhere."""
+        torch = _torch()
+        rates = torch.as_tensor(rates, dtype=torch.float64, device=self._dev()).contiguous()
+        if rates.dim() == 1:
+            rates = rates[None]
+        B = rates.shape[0]
+        w = out if out is not None else torch.empty((B, self.net.N), dtype=torch.float64, device=self._dev())
+        check(lib().esl_mlp_predict(self._h, B, _ptr(rates), _ptr(w)))
+        return w
+
+
 @dataclass
 class SolveResult:
     x_inf: object
@@ -310,8 +434,8 @@ class SolveResult:
     report: Optional[Report] = None
 
 
-def _opts(method: int, tol: float, max_iters: int, max_refine: int, warm=None) -> SolveOpts:
-    return SolveOpts(method, tol, max_iters, max_refine, _ptr(warm))
+def _opts(method: int, tol: float, max_iters: int, max_refine: int, warm=None, occupation=None) -> SolveOpts:
+    return SolveOpts(method, tol, max_iters, max_refine, _ptr(warm), _ptr(occupation))
 
 
 def solve(ctx: Context, net: Net, rates, x0, want_R: bool = False, want_L: bool = False,
@@ -336,8 +460,11 @@ def solve(ctx: Context, net: Net, rates, x0, want_R: bool = False, want_L: bool 
 
 
 def solve_batch(ctx: Context, net: Net, rates, x0, method: int = METHOD_FP64, tol: float = 1e-10,
-                max_iters: int = 0, max_refine: int = 0, warm=None, out=None, marginals: bool = True) -> SolveResult:
-    """B rate sets (B x 2n) x R initial distributions (R x N) -> x_inf (B x R x N)."""
+                max_iters: int = 0, max_refine: int = 0, warm=None, out=None, marginals: bool = True,
+                occupation=None) -> SolveResult:
+    """B rate sets (B x 2n) x R initial distributions (R x N) -> x_inf (B x R x N).
+    ``warm``: optional (B*R) x N device warm start of the occupation; ``occupation``:
+    optional (B*R) x N device output of the expected occupation of transient states."""
     torch = _torch()
     dev = f"cuda:{ctx.device}"
     rates = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
@@ -350,7 +477,7 @@ def solve_batch(ctx: Context, net: Net, rates, x0, method: int = METHOD_FP64, to
     xi = out if out is not None else torch.empty((B, R, net.N), dtype=torch.float64, device=dev)
     mg = torch.empty((B, R, net.n), dtype=torch.float64, device=dev) if marginals else None
     rep = Report()
-    o = _opts(method, tol, max_iters, max_refine, warm)
+    o = _opts(method, tol, max_iters, max_refine, warm, occupation)
     check(lib().esl_solve_batch(ctx._h, net._h, B, _ptr(rates), R, _ptr(x0), _ptr(xi), _ptr(mg), C.byref(o),
                                 C.byref(rep)))
     return SolveResult(xi, mg, report=rep)

@@ -205,6 +205,8 @@ bool sweep_supported(const esl_net* net);
 int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
                   size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st);
 void free_sweep_workspace(void* w);
+// states whose warm start the sweep's grid-wide Krylov groups read (their odd-parity rows)
+int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& states);
 int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                 double* d_x_inf, double* d_marg, double* d_R, double* d_L, const esl_solve_opts* opts,
                 esl_report* rep);

@@ -1557,7 +1557,10 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         o.max_iters = 0;
         o.max_refine = 0;
         o.d_warm = nullptr;
+        o.d_occupation = nullptr;
     }
+    if (o.d_occupation && !((o.method == ESL_METHOD_DIRECT || o.method == ESL_METHOD_MIXED) && sweep_supported(net)))
+        return fail(ESL_ERR_INVALID, "the occupation output needs ESL_METHOD_DIRECT or ESL_METHOD_MIXED and n <= 26");
     if (o.tol <= 0) o.tol = 1e-10;
     if (o.max_iters <= 0) o.max_iters = 600;
     if (o.max_refine <= 0) o.max_refine = 6;
@@ -1656,6 +1659,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     double* y = (double*)ws.get(S_Y, (size_t)K * T * 8, &st_);
     if (st_ != ESL_OK) return st_;
     ESL_CUDA(cudaMemsetAsync(y, 0, (size_t)K * T * 8, s));
+    if (o.d_occupation) ESL_CUDA(cudaMemsetAsync(o.d_occupation, 0, (size_t)K * N * 8, s));
     const bool has_transient = (size_t)TS < N;
     bool swept = false;
     if (has_transient && (o.method == ESL_METHOD_DIRECT || o.method == ESL_METHOD_MIXED) && sweep_supported(net)) {

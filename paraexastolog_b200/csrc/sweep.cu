@@ -927,6 +927,24 @@ __global__ void __launch_bounds__(kSwT) k_sw_term(SwArgs a, int TS, const int32_
     }
 }
 
+// occ[k][state of slot] = Z[slot][k]: a 32 x 32 transpose through shared memory
+__global__ void __launch_bounds__(256) k_sw_occupation(uint32_t M, int K, int Kp, size_t N, const uint2* __restrict__ rows,
+                                                       const double* __restrict__ Z, double* __restrict__ occ) {
+    __shared__ double tile[32][33];
+    __shared__ uint32_t st[32];
+    const uint32_t s0 = blockIdx.x * 32;
+    const int k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (threadIdx.x < 32 && s0 + threadIdx.x < M) st[threadIdx.x] = rows[s0 + threadIdx.x].x;
+    for (int r = ty; r < 32; r += 8)
+        if (s0 + r < M) tile[r][tx] = Z[(size_t)(s0 + r) * Kp + k0 + tx];
+    __syncthreads();
+    for (int c = ty; c < 32; c += 8) {
+        const int k = k0 + c;
+        if (k < K && s0 + tx < M) occ[(size_t)k * N + st[tx]] = tile[tx][c];
+    }
+}
+
 __global__ void k_sw_rate_table(int n, int K, int Kp, int nrhs, const double* __restrict__ rates,
                                 double* __restrict__ rateT) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1130,6 +1148,23 @@ bool debug_on() {
 }  // namespace
 
 void free_sweep_workspace(void* w) { delete static_cast<Workspace*>(w); }
+
+int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& states) {
+    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
+    SweepPlan* P = nullptr;
+    ESL_TRY(build_plan(ctx, net, P));
+    std::vector<uint2> rows(P->M);
+    if (P->M > 0) {
+        ESL_CUDA(cudaMemcpyAsync(rows.data(), P->rows.get(), (size_t)P->M * sizeof(uint2), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    states.clear();
+    for (const SwGroup& g : P->groups)
+        if (g.kind == 2)
+            for (uint32_t r = g.beg + g.ne; r < g.beg + g.ne + g.no; r++) states.push_back(rows[r].x);
+    return ESL_OK;
+}
 
 // slots are packed into 26 bits of a predecessor entry
 bool sweep_supported(const esl_net* net) { return net->n >= 1 && net->n <= 26; }
@@ -1462,6 +1497,13 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         ESL_COUNT_LAUNCH();
         k_sw_term<<<row_grid((uint32_t)P->TS, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
             a, P->TS, net->order.get(), net->term_of.get(), P->tp_ptr.get(), P->tp_ent.get(), x0, x0_ld, Z, T, y);
+        ESL_CUDA(cudaGetLastError());
+    }
+    // expected occupation by state (the learned warm start's training label)
+    if (o.d_occupation && P->M > 0) {
+        ESL_COUNT_LAUNCH();
+        k_sw_occupation<<<dim3((P->M + 31) / 32, Kp / 32), 256, 0, s>>>(P->M, K, Kp, (size_t)net->N, P->rows.get(), Z,
+                                                                        o.d_occupation);
         ESL_CUDA(cudaGetLastError());
     }
     // results of the CTA-local groups

@@ -1,0 +1,173 @@
+"""Learned warm start (esl_mlp_*) and the occupation output, against the CPU oracles.
+
+- occupation z from the level sweep solves (Q - A) z = x0 on the transient states
+  (relative L1 residual <= 1e-8) and is 0 on terminal states;
+- reachability bits are bit-exact against oracle/mlp.reach_bits, features within
+  1e-5 (FP32 logs) of oracle/mlp.features;
+- the loss and gradient of the training kernels match oracle/mlp.loss_grad (float64,
+  same BF16 weights): loss within 1e-4 relative, gradient within 1e-3 in relative norm;
+- the tensor-core inference (BF16 activations) matches the FP32 training forward
+  within 0.05 + 0.02 |y| in standardized log occupation;
+- a trained network's warm start is measured against no warm start on held-out rate
+  sets, and the warm-started solve still matches the oracle (L1 <= 1e-9).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle import mlp as OM
+from paraexastolog_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def esl():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import paraexastolog_b200 as E
+    E.lib()
+    return E
+
+
+@pytest.fixture(scope="module")
+def ctx(esl):
+    return esl.Context(0)
+
+
+@pytest.fixture(scope="module")
+def case(esl, ctx):
+    """n=14 precision-style network with a 1,760-state transient SCC (a grid-wide group)."""
+    w = synth.config_precision(seed=3, n=14, n_rate_sets=256)
+    text = w.networks[0].bnet
+    rates = np.ascontiguousarray(w.rates[0])
+    x0 = np.ascontiguousarray(w.x0[0])
+    model = esl.Model.parse(text)
+    net = esl.Net.build(ctx, model, rates[0])
+    om = O.Model(text=text)
+    sym = om.analyse(rates[0])
+    F = om.flip_masks(rates[0])
+    return dict(text=text, rates=rates, x0=x0, model=model, net=net, om=om, sym=sym, F=F, n=14)
+
+
+def _transient(sym):
+    term = np.zeros(sym.N, bool)
+    term[sym.order[: sym.offsets[sym.T]]] = True
+    return ~term
+
+
+def test_occupation_solves_the_transient_system(esl, ctx, case):
+    n, N, F = case["n"], 1 << case["n"], case["F"]
+    rates = case["rates"][:4]
+    occ = torch.empty((4, N), dtype=torch.float64, device="cuda")
+    esl.solve_batch(ctx, case["net"], rates, case["x0"], method=esl.METHOD_DIRECT, tol=1e-12, occupation=occ)
+    z = occ.cpu().numpy()
+    tr = _transient(case["sym"])
+    assert np.all(z[:, ~tr] == 0.0)
+    assert np.all(z[:, tr] > 0.0)
+    v = np.arange(N)
+    for k in range(4):
+        r = rates[k]
+        out = np.zeros(N)
+        inflow = np.zeros(N)
+        for i in range(n):
+            has = ((F >> i) & 1).astype(bool)
+            rate = r[2 * i + ((v >> i) & 1)]
+            out += np.where(has, rate, 0.0)
+            src = v[has & tr]
+            np.add.at(inflow, src ^ (1 << i), rate[src] * z[k, src])
+        res = out * z[k] - inflow - case["x0"][0]
+        rel = np.abs(res[tr]).sum() / np.abs(case["x0"][0][tr]).sum()
+        assert rel <= 1e-8, (k, rel)
+
+
+def test_reach_and_features(esl, ctx, case):
+    mlp = esl.Mlp(ctx, case["net"], seed=1)
+    assert mlp.n_targets > 0
+    reach_ref = OM.reach_bits(case["sym"], case["F"])
+    reach = mlp.reach().cpu().numpy().astype(np.uint32)
+    assert np.array_equal(reach, reach_ref)
+    rng = np.random.default_rng(0)
+    tg = mlp.targets().cpu().numpy()
+    vs = rng.choice(tg, 300)
+    ks = rng.integers(0, 256, 300)
+    X = mlp.features(case["rates"], ks, vs).cpu().numpy()
+    Xr = OM.features(14, case["sym"].T, case["F"], reach_ref, case["rates"], ks, vs)
+    assert np.all(X[:, 77:] == 0.0)
+    assert np.abs(X[:, :77] - Xr).max() <= 1e-5
+
+
+def test_gradient_matches_oracle(esl, ctx, case):
+    mlp = esl.Mlp(ctx, case["net"], seed=7)
+    rng = np.random.default_rng(3)
+    tg = mlp.targets().cpu().numpy()
+    S = 512
+    vs = rng.choice(tg, S)
+    ks = rng.integers(0, 256, S)
+    t = rng.normal(0, 1, S).astype(np.float32)
+    p = mlp.get_params()
+    p[OM.N_PARAMS - 129:OM.N_PARAMS - 1] += 0.05  # non-trivial head
+    mlp.set_params(p, 0.0, 1.0)
+    loss, g = mlp.loss_grad(case["rates"], ks, vs, t)
+    X = OM.features(14, case["sym"].T, case["F"], OM.reach_bits(case["sym"], case["F"]), case["rates"], ks, vs)
+    lr, gr = OM.loss_grad(p, X, t)
+    assert abs(loss - lr) <= 1e-4 * abs(lr), (loss, lr)
+    err = np.linalg.norm(g - gr) / np.linalg.norm(gr)
+    assert err <= 1e-3, err
+    # every parameter block receives its own gradient
+    for name, shape in OM.SIZES:
+        blk = OM.unpack(g)[name]
+        assert np.any(blk != 0.0), name
+
+
+def test_tensor_core_inference_matches_forward(esl, ctx, case):
+    mlp = esl.Mlp(ctx, case["net"], seed=11)
+    p = mlp.get_params()
+    mlp.set_params(p, 0.0, 1.0)
+    rates = case["rates"][:40]
+    warm = mlp.predict(rates)
+    tg = mlp.targets().cpu().numpy()
+    rng = np.random.default_rng(5)
+    vs = rng.choice(tg, 2000)
+    ks = rng.integers(0, 40, 2000)
+    y = mlp.forward(rates, ks, vs).cpu().numpy().astype(np.float64)
+    w = warm.cpu().numpy()
+    yp = np.log(w[ks, vs])
+    assert np.all(np.isfinite(yp))
+    assert np.all(np.abs(yp - y) <= 0.05 + 0.02 * np.abs(y)), np.abs(yp - y).max()
+    # zero outside the targets
+    mask = np.ones(case["net"].N, bool)
+    mask[tg] = False
+    assert np.all(w[:, mask] == 0.0)
+
+
+def test_trained_warm_start_gain(esl, ctx, case, capsys):
+    rates = case["rates"]
+    train, held = rates[:192], rates[192:]
+    net = case["net"]
+    occ = torch.empty((192, net.N), dtype=torch.float64, device="cuda")
+    esl.solve_batch(ctx, net, train, case["x0"], method=esl.METHOD_DIRECT, tol=1e-12, occupation=occ,
+                    marginals=False)
+    mlp = esl.Mlp(ctx, net, seed=3)
+    loss0 = mlp.train(train, occ, steps=1, batch=8192, lr=2e-3)
+    loss = mlp.train(train, occ, steps=800, batch=8192, lr=2e-3)
+    assert loss < 0.5 * loss0, (loss0, loss)
+    cold = esl.solve_batch(ctx, net, held, case["x0"], method=esl.METHOD_MIXED, tol=1e-10)
+    warm = mlp.predict(held)
+    hot = esl.solve_batch(ctx, net, held, case["x0"], method=esl.METHOD_MIXED, tol=1e-10, warm=warm)
+    ref, _ = case["sym"].solve_many(held[:4], np.stack([case["x0"][0]] * 4), threads=4)
+    xi = hot.x_inf[:4, 0].cpu().numpy()
+    assert np.abs(xi - ref.reshape(4, -1)).sum(1).max() <= 1e-9
+    # relative error of the prediction on the targets
+    occ_h = torch.empty((64, net.N), dtype=torch.float64, device="cuda")
+    esl.solve_batch(ctx, net, held, case["x0"], method=esl.METHOD_DIRECT, tol=1e-12, occupation=occ_h,
+                    marginals=False)
+    tg = mlp.targets().long()
+    lerr = (torch.log(warm[:, tg]) - torch.log(occ_h[:, tg])).abs()
+    with capsys.disabled():
+        print(f"\n[warm start] train loss {loss0:.3f} -> {loss:.4f}; held-out |log z error| median "
+              f"{lerr.median().item():.3f} p90 {lerr.quantile(0.9).item():.3f}; Krylov iterations "
+              f"cold {cold.report.iterations} warm {hot.report.iterations}")
+    assert hot.report.converged == 1
