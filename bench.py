@@ -9,7 +9,13 @@ ranks (max device time over ranks); `e2e` = the same through the public Python A
 with pinned host inputs copied in and the results (marginals + terminal-state
 probabilities, i.e. every nonzero of x_inf) copied back inside the timed region.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--method fp64|mixed|direct]
+The metric compares the learned-warm-start + mixed-precision form with the plain FP64
+form.  The headline (`--method direct`, default) is the plain FP64 level sweep, the
+faster of the two on this workload; the learned+mixed form is timed the same way in
+the same run (`learned_mixed`), after its network is trained outside the timed region
+on the plain solves' occupations of the 3,584 training rate sets.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--method direct|learned|mixed|fp64]
     python bench.py --impl reference ...   # the CPU FP64 oracle on the host cores
 
 Synthetic data: seeded random network (paraexastolog_b200.synth), no dataset.
@@ -36,14 +42,38 @@ METRIC = "solves/s, n=20 x 512 rate sets, learned+mixed vs FP64 sparse LU at L1<
 BATCH = 512
 
 
+N_TRAIN = 3584
+
+
 def workload(rank: int):
+    """(network, held-out rate sets of this rank, x0, training rate sets)."""
     w = synth.config_learned(n_rate_sets=4096)
     net = w.networks[0]
     rates = w.rates[0][-BATCH:]
     if rank > 0:  # weak scaling: further seeded rate sets of the same distribution
         rng = np.random.default_rng(10_000 + rank)
         rates = synth.log_uniform_rates(rng, net.n, BATCH)
-    return net, np.ascontiguousarray(rates), np.ascontiguousarray(w.x0[0])
+    return (net, np.ascontiguousarray(rates), np.ascontiguousarray(w.x0[0]),
+            np.ascontiguousarray(w.rates[0][:N_TRAIN]))
+
+
+def train_warm_start(esl, torch, ctx, net, x0, train_rates, steps: int, device: int):
+    """Outside the timed region: plain FP64 (direct) occupations of the training rate sets,
+    in chunks of BATCH, each followed by Adam steps of the warm-start network on it."""
+    mlp = esl.Mlp(ctx, net, seed=0)
+    occ = torch.empty((BATCH, net.N), dtype=torch.float64, device=f"cuda:{device}")
+    t0 = time.perf_counter()
+    chunks = (len(train_rates) + BATCH - 1) // BATCH
+    loss = None
+    for c in range(chunks):
+        r = train_rates[c * BATCH:(c + 1) * BATCH]
+        esl.solve_batch(ctx, net, r, x0, method=esl.METHOD_DIRECT, tol=1e-10, occupation=occ[: len(r)],
+                        marginals=False)
+        loss = mlp.train(r, occ[: len(r)], steps=steps // chunks, batch=16384, lr=2e-3)
+    torch.cuda.synchronize(device)
+    del occ
+    return mlp, {"train_rate_sets": len(train_rates), "adam_steps": steps // chunks * chunks, "batch": 16384,
+                 "final_loss": loss, "seconds": time.perf_counter() - t0, "targets": mlp.n_targets}
 
 
 def peaks():
@@ -121,16 +151,24 @@ def run_ours(args, rank, world, device):
     torch.cuda.set_device(device)
     stream = torch.cuda.current_stream(device)
     ctx = esl.Context(device, stream)
-    net_g, rates, x0 = workload(rank)
-    method = {"fp64": esl.METHOD_FP64, "mixed": esl.METHOD_MIXED, "direct": esl.METHOD_DIRECT}[args.method]
+    net_g, rates, x0, train_rates = workload(rank)
     model = esl.Model.parse(net_g.bnet)
     d_rates = torch.tensor(rates, device=f"cuda:{device}")
     d_x0 = torch.tensor(x0, device=f"cuda:{device}")
     N = 1 << model.n
+    learned = args.method == "learned"
+    solve_method = {"fp64": esl.METHOD_FP64, "mixed": esl.METHOD_MIXED, "direct": esl.METHOD_DIRECT,
+                    "learned": esl.METHOD_MIXED}[args.method]
+    mlp, train_info, warm_buf = None, None, None
+    if learned or not args.no_compare:
+        net0 = esl.Net.build(ctx, model, rates[0])
+        mlp, train_info = train_warm_start(esl, torch, ctx, net0, x0, train_rates, args.train_steps, device)
+        warm_buf = torch.empty((BATCH, N), dtype=torch.float64, device=f"cuda:{device}")
 
-    def step():
+    def step(method=solve_method, use_warm=learned, dr=d_rates, dx=d_x0):
         net = esl.Net.build(ctx, model, rates[0])
-        res = esl.solve_batch(ctx, net, d_rates, d_x0, method=method, tol=args.tol)
+        warm = mlp.predict(dr, out=warm_buf) if use_warm else None
+        res = esl.solve_batch(ctx, net, dr, dx, method=method, tol=args.tol, warm=warm)
         return net, res
 
     def barrier():
@@ -138,22 +176,48 @@ def run_ours(args, rank, world, device):
             dist.barrier()
         torch.cuda.synchronize(device)
 
+    def timed(fn, steps):
+        barrier()
+        l0 = esl.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(device) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                out = fn()
+            e1.record(stream)
+            barrier()
+        return out, e0.elapsed_time(e1), esl.launch_count() - l0, clk.summary()
+
     for _ in range(args.warmup):
         net, res = step()
-    # device-resident timed region
-    barrier()
-    launches0 = esl.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(device) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            net, res = step()
-        e1.record(stream)
-        barrier()
-    launches = esl.launch_count() - launches0
-    ms = e0.elapsed_time(e1)
-    clocks = clk.summary()
+    (net, res), ms, launches, clocks = timed(step, args.steps)
     iters, relres = res.report.iterations, res.report.relres
+    last_xinf = res.x_inf
+
+    # the other form of the metric's comparison, timed the same way on the same GPU and batch:
+    # learned warm start + mixed precision when the headline is the plain FP64 form, and the
+    # plain FP64 form otherwise
+    other = None
+    if not args.no_compare:
+        if learned or args.method != "direct":
+            o_step = lambda: step(method=esl.METHOD_DIRECT, use_warm=False)  # noqa: E731
+            o_name = "direct"
+        else:
+            o_step = lambda: step(method=esl.METHOD_MIXED, use_warm=True)  # noqa: E731
+            o_name = "learned+mixed"
+        for _ in range(max(1, args.warmup - 1)):
+            o_step()
+        (_, ores), oms, _, _ = timed(o_step, args.steps)
+        other = {"method": o_name, "value": BATCH * args.steps * world / (oms * 1e-3),
+                 "ms_per_step": oms / args.steps, "iterations": ores.report.iterations,
+                 "relres": ores.report.relres}
+        if mlp is not None:
+            # iterations of the mixed solve without the warm start, and the inference time alone
+            cres = esl.solve_batch(ctx, net, d_rates, d_x0, method=esl.METHOD_MIXED, tol=args.tol)
+            other["mixed_without_warm_start_iterations"] = cres.report.iterations
+            _, pms, _, _ = timed(lambda: mlp.predict(d_rates, out=warm_buf), 3)
+            other["warm_start_inference_ms"] = pms / 3
+            other["warm_start_training"] = train_info
 
     # roofline of the dominant kernel pair (Schur operator) from live CUDA events
     ctx.set_profiling(True)
@@ -172,12 +236,10 @@ def run_ours(args, rank, world, device):
     f0.record(stream)
     t_wall = time.perf_counter()
     for _ in range(args.steps):
-        m = esl.Model.parse(net_g.bnet)
         dr = h_rates.to(f"cuda:{device}", non_blocking=True)
         dx = h_x0.to(f"cuda:{device}", non_blocking=True)
         h2d = dr.numel() * 8 + dx.numel() * 8
-        net = esl.Net.build(ctx, m, rates[0])
-        res = esl.solve_batch(ctx, net, dr, dx, method=method, tol=args.tol)
+        net, res = step(dr=dr, dx=dx)
         if term_idx is None:
             order, _, _, _ = net.export()
             term_idx = order[: net.terminal_states].long()
@@ -199,9 +261,10 @@ def run_ours(args, rank, world, device):
         peak, peak_kind = peaks()
         achieved = op_bytes / (op_ms * 1e-3) / 1e9 if op_ms > 0 else None
         tpb = traffic_per_byte()
+        value = solves / (ms * 1e-3)
         out = {
             "metric": METRIC,
-            "value": solves / (ms * 1e-3),
+            "value": value,
             "unit": "solves/s",
             "n_gpus": world,
             "steps": args.steps,
@@ -210,14 +273,16 @@ def run_ours(args, rank, world, device):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64" if args.method != "mixed" else "f32+f64",
+            "dtype": {"direct": "f64", "fp64": "f64"}.get(args.method, "f32+f64"),
             "data": "synthetic (seeded random Boolean network, log-uniform rates)",
             "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "n_nodes": model.n,
                        "states": N, "batch_rate_sets": BATCH, "initial_distributions": 1,
-                       "method": args.method, "tol_relres": args.tol,
+                       "method": "learned+mixed" if learned else args.method, "tol_relres": args.tol,
                        "l2": "working set > L2 (x_inf alone is 4 GB per step)",
                        "parallelism": f"replicas x{world} (rate-set shards)",
-                       "step": "table + SCC/levels/order + terminal kernels + transient solve + x_inf/marginals"},
+                       "step": ("table + SCC/levels/order + terminal kernels + " +
+                                ("warm-start inference + " if learned else "") +
+                                "transient solve + x_inf/marginals")},
             "e2e": {"value": solves / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "wall_s": e2e_wall},
             "gpu_launches": int(launches),
@@ -231,24 +296,28 @@ def run_ours(args, rank, world, device):
             "solver": {"iterations": iters, "relres": relres},
             "clocks": clocks,
         }
-    return out
+        if other:
+            other["value_over_headline"] = other["value"] / value
+            out["learned_mixed" if other["method"] == "learned+mixed" else "plain_fp64"] = other
+    return out, last_xinf
 
 
 def cpu_baseline(sample: int):
-    """The CPU FP64 oracle on this host's cores over a bounded sample of rate sets."""
+    """The CPU FP64 oracle on this host's cores over a bounded sample of rate sets;
+    returns (baseline record, seconds, the oracle's x_inf of the sample)."""
     import oracle as O
 
-    net_g, rates, x0 = workload(0)
+    net_g, rates, x0, _ = workload(0)
     m = O.Model(text=net_g.bnet)
     sym = m.analyse(rates[0])
     threads = min(os.cpu_count() or 1, sample)
     r = rates[:sample]
     xs = np.broadcast_to(x0, (sample, x0.size)).copy()
     t = time.perf_counter()
-    sym.solve_many(r, xs, threads=threads)
+    ref, _ = sym.solve_many(r, xs, threads=threads)
     dt = time.perf_counter() - t
     return {"value": sample / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"{sample} of the 512 held-out rate sets, oracle symbolic analysis excluded"}, dt
+            "sample": f"{sample} of the 512 held-out rate sets, oracle symbolic analysis excluded"}, dt, ref
 
 
 def run_reference(args):
@@ -257,7 +326,7 @@ def run_reference(args):
         cpu_baseline(sample)
     total, solves = 0.0, 0
     for _ in range(args.steps):
-        cb, dt = cpu_baseline(sample)
+        cb, dt, _ = cpu_baseline(sample)
         total += dt
         solves += sample
     value = solves / total
@@ -276,7 +345,12 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="direct", choices=["direct", "fp64", "mixed"])
+    ap.add_argument("--method", default="direct", choices=["direct", "learned", "mixed", "fp64"],
+                    help="headline form: direct = plain FP64 level sweep (the fastest here); "
+                         "learned = learned warm start + mixed precision")
+    ap.add_argument("--train-steps", type=int, default=1400, help="Adam steps of the warm-start network")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the other form of the comparison (learned+mixed vs plain FP64)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -296,10 +370,16 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    out = run_ours(args, rank, world, local)
+    out, xinf = run_ours(args, rank, world, local)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            out["cpu_baseline"], _ = cpu_baseline(max(8, min(os.cpu_count() or 8, 16)))
+            sample = max(8, min(os.cpu_count() or 8, 16))
+            out["cpu_baseline"], _, ref = cpu_baseline(sample)
+            # error of this run's results against the FP64 oracle on the sampled rate sets
+            got = xinf[:sample, 0].cpu().numpy()
+            diff = np.abs(got - ref.reshape(sample, -1))
+            out["accuracy_vs_fp64_oracle"] = {"rate_sets": sample, "l1_max": float(diff.sum(1).max()),
+                                              "maxabs": float(diff.max()), "target_l1": 1e-9}
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -28,6 +28,7 @@
 // read once per row and shared by every system.  Rates are staged per CTA in shared
 // memory as [rate index][system lane].
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -329,6 +330,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
 //   MODE 1: Y = B - y                    (true residual, FP64), acc0 += Y^2
 //   MODE 2: Y = y                        acc0 += AUX . Y   (AUX = r0)
 //   MODE 3: Y = y                        acc0 += Y . (AUX X), acc1 += Y . Y   (AUX = dS)
+//   MODE 4: (no output)                  acc0 += y . B, acc1 += y . y   (B = reduced rhs)
 // S systems per thread.  X, AUX and Y are streamed (evict-first) so that the gathered W
 // keeps its place in L2.
 template <int S, int MODE, class T>
@@ -379,6 +381,9 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
                     } else if (MODE == 2) {
                         __stcs(Y + i, y);
                         d0[q] += (double)__ldcs(AUX + i) * (double)y;
+                    } else if (MODE == 4) {
+                        d0[q] += (double)y * B[i];
+                        d1[q] += (double)y * (double)y;
                     } else {
                         __stcs(Y + i, y);
                         d0[q] += (double)y * ((double)__ldcs(AUX + i) * (double)x);
@@ -388,7 +393,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
             }
         }
     }
-    if (MODE == 3) {
+    if (MODE == 3 || MODE == 4) {
         double v[2][S];
 #pragma unroll
         for (int q = 0; q < S; q++) {
@@ -591,6 +596,17 @@ __global__ void __launch_bounds__(kSwT) k_sw_init(SwArgs a, const double* __rest
             x = warm ? warm[(size_t)t.k * warm_ld + a.rows[slot].x] : 0.0;
         X64[idx] = x;
     }
+}
+
+// X *= alpha_k = (S X . b) / (S X . S X): the least-squares multiple of the warm start,
+// whose residual is never larger than that of a zero start
+__global__ void __launch_bounds__(kSwT) k_sw_warm_scale(SwArgs a, const double* __restrict__ yb,
+                                                        const double* __restrict__ yy, double* __restrict__ X64) {
+    const Tile t = tile_of(a.KT);
+    if (t.k >= a.K) return;
+    const double alpha = yy[t.k] > 0.0 ? yb[t.k] / yy[t.k] : 0.0;
+    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB)
+        X64[(size_t)r * a.Kp + t.k] *= alpha;
 }
 
 // ---- CTA-local refinement for groups of small SCCs ----------------------------------------
@@ -1118,6 +1134,18 @@ size_t tile_bytes() {
     return b;
 }
 
+// Relative residual target of an FP32 inner solve of the grid-wide groups, a tuning
+// parameter (ESL_MIXED_INNER_REL, default 1e-5).
+double mixed_inner_rel() {
+    static double r = 0.0;
+    if (r == 0.0) {
+        const char* e = getenv("ESL_MIXED_INNER_REL");
+        const double v = e ? atof(e) : 0.0;
+        r = (v > 0.0 && v < 1.0) ? v : 1e-5;
+    }
+    return r;
+}
+
 int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0) {
     int kt = 128;
     while (kt > 32 && (Kp % kt != 0 || (size_t)2 * n * kt * elem > 40 * 1024 ||
@@ -1220,6 +1248,15 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
     int total_iters = 0;
 
     for (const SwGroup& g : P->groups) {
+        // debug timing: wall time of the group with the stream drained on both sides
+        std::chrono::steady_clock::time_point g_t0;
+        if (debug_on()) {
+            ESL_CUDA(cudaStreamSynchronize(s));
+            g_t0 = std::chrono::steady_clock::now();
+        }
+        auto g_ms = [&]() {
+            return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_t0).count();
+        };
         a.beg = g.beg;
         a.ne = g.ne;
         a.no = g.no;
@@ -1341,8 +1378,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 }
                 fprintf(stderr,
                         "[esl-sweep] local group beg %u even %u odd %u max_scc %d sccs %u warps %d: failed %d "
-                        "worst relres so far %.3e\n",
-                        g.beg, g.ne, g.no, g.max_scc, g.nscc, nw, nf, std::sqrt(worst));
+                        "worst relres so far %.3e, %.3f ms\n",
+                        g.beg, g.ne, g.no, g.max_scc, g.nscc, nw, nf, std::sqrt(worst), g_ms());
             }
             continue;
         }
@@ -1357,11 +1394,24 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         };
+        if (o.d_warm) {
+            // least-squares scale of the warm start per system (C_R0V, C_TS as scratch)
+            ESL_CUDA(cudaMemsetAsync(sc.c[C_R0V], 0, (size_t)Kp * 8, s));
+            ESL_CUDA(cudaMemsetAsync(sc.c[C_TS], 0, (size_t)Kp * 8, s));
+            ESL_COUNT_LAUNCH();
+            k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
+            ESL_COUNT_LAUNCH();
+            k_sw_apply<1, 4, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, nullptr, sc.c[C_R0V],
+                                                              sc.c[C_TS]);
+            ESL_COUNT_LAUNCH();
+            k_sw_warm_scale<<<go, kSwT, 0, s>>>(a, sc.c[C_R0V], sc.c[C_TS], X64);
+            ESL_CUDA(cudaGetLastError());
+        }
         ESL_TRY(true_residual());
         bool inner64 = !mixed;
         int group_iters = 0;
         for (int outer = 0;; outer++) {
-            const double inner_rel = inner64 ? 1e-13 : 1e-5;
+            const double inner_rel = inner64 ? 1e-13 : mixed_inner_rel();
             ESL_COUNT_LAUNCH();
             k_sw_outer<<<1, 1024, 0, s>>>(K, sc, tol * tol, inner_rel * inner_rel, kSwAcceptRel * kSwAcceptRel,
                                           outer, max_refine, d_cnt);
@@ -1487,8 +1537,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         st.relres = std::max(st.relres, worst);
         total_iters += group_iters;
         if (debug_on())
-            fprintf(stderr, "[esl-sweep] group beg %u even %u odd %u max_scc %d: iters %d relres %.3e\n", g.beg, g.ne,
-                    g.no, g.max_scc, group_iters, worst);
+            fprintf(stderr, "[esl-sweep] group beg %u even %u odd %u max_scc %d: iters %d relres %.3e, %.3f ms\n",
+                    g.beg, g.ne, g.no, g.max_scc, group_iters, worst, g_ms());
     }
     // masses into the terminal SCCs
     a.flags = nullptr;
