@@ -16,6 +16,7 @@ static thread_local std::string g_error;
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_error = msg; }
 int fail(int code, const std::string& msg) {

@@ -31,6 +31,7 @@ int fail(int code, const std::string& msg);
 
 // ---- launch accounting: every kernel launch of the library is counted --------
 void count_launch();
+void count_launches(uint64_t n);  // kernels of a replayed CUDA graph
 #define ESL_COUNT_LAUNCH() ::esl::count_launch()
 
 // ---- host model -------------------------------------------------------------

@@ -1167,6 +1167,21 @@ dim3 row_grid(uint32_t rows, int Kp, int KT, int sm_count, int S = 1) {
     return dim3((unsigned)want, ty);
 }
 
+// the two graphs (one per poll-slot parity) of a Krylov solve, released on scope exit
+struct GraphPair {
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    GraphPair() = default;
+    GraphPair(const GraphPair&) = delete;
+    GraphPair& operator=(const GraphPair&) = delete;
+    ~GraphPair() {
+        for (int p = 0; p < 2; p++) {
+            if (exec[p]) cudaGraphExecDestroy(exec[p]);
+            if (graph[p]) cudaGraphDestroy(graph[p]);
+        }
+    }
+};
+
 bool debug_on() {
     static int on = -1;
     if (on < 0) on = getenv("ESL_DEBUG") ? 1 : 0;
@@ -1445,54 +1460,82 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                                         12.0 * (g.ne + g.no) + 4.0 * (double)g.nin;
                 ESL_COUNT_LAUNCH();
                 k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, R, R0, D, PH, V);
-                int it = 0, chunk = 0;
-                for (; it < max_iters; it += kSwPoll, chunk++) {
+                // kSwPoll iterations; `par` picks the running-count slot of this poll window
+                auto launch_chunk = [&](int par, bool record) -> int {
                     for (int j = 0; j < kSwPoll; j++) {
-                        ESL_COUNT_LAUNCH();
-                        k_sw_p<TT><<<goi, kSwT, 0, s>>>(a, sc, R, dS, V, PH);
-                        const bool rec = ctx->prof && chunk == 0;
-                        cudaEvent_t ea = nullptr, eb = nullptr;
-                        if (rec) {
-                            ea = ctx->prof_event();
-                            eb = ctx->prof_event();
-                            ESL_CUDA(cudaEventRecord(ea, s));
-                        }
-                        ESL_COUNT_LAUNCH();
-                        if (s2)
-                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
-                        else
-                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
-                        ESL_COUNT_LAUNCH();
-                        if (s2)
-                            k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
-                        else
-                            k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
-                        if (rec) {
-                            ESL_CUDA(cudaEventRecord(eb, s));
-                            ctx->prof_recs.push_back({ea, eb, op_bytes});
-                        }
-                        ESL_COUNT_LAUNCH();
-                        k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
-                        ESL_COUNT_LAUNCH();
-                        if (s2)
-                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, SH, WW);
-                        else
-                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
-                        ESL_COUNT_LAUNCH();
-                        if (s2)
-                            k_sw_apply<2, 3, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                          sc.c[C_TT]);
-                        else
-                            k_sw_apply<1, 3, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                          sc.c[C_TT]);
-                        ESL_COUNT_LAUNCH();
-                        k_sw_xr<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, D, R);
-                        ESL_COUNT_LAUNCH();
-                        k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, d_cnt + 1 + (chunk & 1));
+                    ESL_COUNT_LAUNCH();
+                    k_sw_p<TT><<<goi, kSwT, 0, s>>>(a, sc, R, dS, V, PH);
+                    const bool rec = record;
+                    cudaEvent_t ea = nullptr, eb = nullptr;
+                    if (rec) {
+                        ea = ctx->prof_event();
+                        eb = ctx->prof_event();
+                        ESL_CUDA(cudaEventRecord(ea, s));
+                    }
+                    ESL_COUNT_LAUNCH();
+                    if (s2)
+                        k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                    else
+                        k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                    ESL_COUNT_LAUNCH();
+                    if (s2)
+                        k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                    else
+                        k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                    if (rec) {
+                        ESL_CUDA(cudaEventRecord(eb, s));
+                        ctx->prof_recs.push_back({ea, eb, op_bytes});
+                    }
+                    ESL_COUNT_LAUNCH();
+                    k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                    ESL_COUNT_LAUNCH();
+                    if (s2)
+                        k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                    else
+                        k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                    ESL_COUNT_LAUNCH();
+                    if (s2)
+                        k_sw_apply<2, 3, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                      sc.c[C_TT]);
+                    else
+                        k_sw_apply<1, 3, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                      sc.c[C_TT]);
+                    ESL_COUNT_LAUNCH();
+                    k_sw_xr<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, D, R);
+                    ESL_COUNT_LAUNCH();
+                    k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, d_cnt + 1 + par);
                     }
                     ESL_CUDA(cudaGetLastError());
-                    ESL_CUDA(cudaMemcpyAsync(h_cnt + 1 + (chunk & 1), d_cnt + 1 + (chunk & 1), 4,
-                                             cudaMemcpyDeviceToHost, s));
+                    return ESL_OK;
+                };
+                // After the first poll window the launches of a window are replayed from a
+                // CUDA graph (one per slot parity): the small level groups are bound by the
+                // host's launch rate, not by the GPU.
+                GraphPair gp;
+                cudaGraph_t* graph = gp.graph;
+                cudaGraphExec_t* gexec = gp.exec;
+                int it = 0, chunk = 0;
+                for (; it < max_iters; it += kSwPoll, chunk++) {
+                    const int par = chunk & 1;
+                    if (chunk == 0) {
+                        ESL_TRY(launch_chunk(par, ctx->prof));
+                    } else if (!gexec[par]) {
+                        int rc = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess
+                                     ? launch_chunk(par, false)
+                                     : fail(ESL_ERR_CUDA, "stream capture failed to start");
+                        if (cudaStreamEndCapture(s, &graph[par]) != cudaSuccess && rc == ESL_OK)
+                            rc = fail(ESL_ERR_CUDA, "stream capture failed");
+                        if (rc == ESL_OK && cudaGraphInstantiate(&gexec[par], graph[par], 0) != cudaSuccess)
+                            rc = fail(ESL_ERR_CUDA, "graph instantiation failed");
+                        if (rc == ESL_OK && cudaGraphLaunch(gexec[par], s) != cudaSuccess)
+                            rc = fail(ESL_ERR_CUDA, "graph launch failed");
+                        if (rc != ESL_OK) return rc;
+                    } else {
+                        count_launches(8 * kSwPoll);
+                        if (cudaGraphLaunch(gexec[par], s) != cudaSuccess)
+                            return fail(ESL_ERR_CUDA, "graph launch failed");
+                    }
+                    ESL_CUDA(cudaMemcpyAsync(h_cnt + 1 + par, d_cnt + 1 + par, 4, cudaMemcpyDeviceToHost, s));
                     ESL_CUDA(cudaEventRecord(ctx->poll_ev[chunk & 1], s));
                     if (chunk >= 1) {
                         ESL_CUDA(cudaEventSynchronize(ctx->poll_ev[(chunk - 1) & 1]));
