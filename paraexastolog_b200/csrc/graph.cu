@@ -19,6 +19,10 @@
 // level and reversal produce (cuda/src/transition_graph.cu:151-184) -- with the
 // states of an SCC ascending.
 // Every fixpoint loop runs under an iteration budget and fails with ESL_ERR_TIMEOUT.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
@@ -225,6 +229,7 @@ __global__ void k_domain_masks(int n, uint64_t N, const uint32_t* __restrict__ F
 
 struct Flags {
     esl_ctx* ctx;
+    int64_t reads = 0;
     int reset() {
         ESL_CUDA(cudaMemsetAsync(ctx->d_flag.get(), 0, 8 * sizeof(unsigned long long), ctx->stream));
         return ESL_OK;
@@ -234,6 +239,7 @@ struct Flags {
         return ESL_OK;
     }
     int read(unsigned long long* out, int count) {
+        reads++;
         ESL_CUDA(cudaMemcpyAsync(ctx->h_flag, ctx->d_flag.get(), count * sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, ctx->stream));
         ESL_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -265,6 +271,11 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     const uint32_t* F = net->F.get();
     const uint32_t* G = net->G.get();
     Flags fl{ctx};
+    const bool dbg = getenv("ESL_DEBUG") != nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms_since = [&]() {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
     // budgets: a sweep can only fail to progress once per state
     const int64_t budget = (int64_t)N + 64;
 
@@ -317,6 +328,8 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         ESL_TRY(trim());
         ESL_TRY(fl.read(st, 2));
     }
+    if (dbg) fprintf(stderr, "[esl-graph] SCC: %lld rounds, %lld flag reads, %.1f ms\n", (long long)rounds,
+                     (long long)fl.reads, ms_since());
     // canonical labels: smallest state of each SCC
     ESL_TRY(canon.alloc(N));
     ESL_COUNT_LAUNCH();
@@ -415,6 +428,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     k_domain_masks<<<nb, kThreads, 0, s>>>(n, N, F, G, net->term_of.get(), net->Fdom.get(), net->Gdom.get());
     ESL_CUDA(cudaGetLastError());
     ESL_CUDA(cudaStreamSynchronize(s));
+    if (dbg) fprintf(stderr, "[esl-graph] done: %lld flag reads, %.1f ms\n", (long long)fl.reads, ms_since());
     return ESL_OK;
 }
 

@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "esl_internal.h"
@@ -973,12 +974,15 @@ __global__ void k_sw_rate_table(int n, int K, int Kp, int nrhs, const double* __
 enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R, W_R0, W_PH, W_V, W_SH, W_TT,
               W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_F0, W_COUNT = W_F0 + 8 };
 
+bool debug_on();
+
 int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     if (net->sweep) {
         out = static_cast<SweepPlan*>(net->sweep);
         return ESL_OK;
     }
     cudaStream_t s = ctx->stream;
+    const auto t_start = std::chrono::steady_clock::now();
     const size_t N = (size_t)net->N;
     const int n_sccs = net->n_sccs, T = net->T;
     std::vector<int32_t> order(N), offsets(n_sccs + 1), levels(std::max(n_sccs, 1)), term_of(N);
@@ -1049,30 +1053,64 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
         P->groups.push_back(g);
         c = c1;
     }
-    // predecessor lists
-    std::vector<uint32_t> ig_ptr{0}, og_ptr{0}, ig, og;
-    ig_ptr.reserve(M + 1);
-    og_ptr.reserve(M + 1);
-    for (SwGroup& g : P->groups) {
-        const size_t ig0 = ig.size();
-        const uint32_t end = g.beg + g.ne + g.no;
-        for (uint32_t sl = g.beg; sl < end; sl++) {
-            const uint32_t v = rows[sl].x;
-            uint32_t in = G[v];
-            while (in) {
-                const int i = __builtin_ctz(in);
-                in &= in - 1;
-                const uint32_t su = slot_of[v ^ (1u << i)];
-                if (su == 0xFFFFFFFFu) continue;  // a terminal state has no edge out of its SCC
-                // source bit i is the complement of v's
-                const uint32_t ri = 2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u);
-                ((su >= g.beg && su < end) ? ig : og).push_back((su << 6) | ri);
-            }
-            ig_ptr.push_back((uint32_t)ig.size());
-            og_ptr.push_back((uint32_t)og.size());
+    // Predecessor lists, built by host threads in two passes over slot ranges (count,
+    // then fill at the prefix offsets) so that the entries come out in slot order.
+    std::vector<uint32_t> gend(M);  // end slot of each slot's group
+    for (const SwGroup& g : P->groups)
+        for (uint32_t sl = g.beg; sl < g.beg + g.ne + g.no; sl++) gend[sl] = g.beg + g.ne + g.no;
+    std::vector<uint32_t> gbeg(M);
+    for (const SwGroup& g : P->groups)
+        for (uint32_t sl = g.beg; sl < g.beg + g.ne + g.no; sl++) gbeg[sl] = g.beg;
+    std::vector<uint32_t> ig_ptr(M + 1, 0), og_ptr(M + 1, 0), ig, og;
+    const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    auto for_slots = [&](auto fn) {
+        std::vector<std::thread> th;
+        const uint32_t per = (M + nth - 1) / nth;
+        for (int t = 0; t < nth; t++) {
+            const uint32_t a0 = std::min<uint32_t>(M, t * per), a1 = std::min<uint32_t>(M, a0 + per);
+            th.emplace_back([=, &fn]() { fn(a0, a1); });
         }
-        g.nin = ig.size() - ig0;
+        for (auto& x : th) x.join();
+    };
+    auto visit = [&](uint32_t sl, auto emit) {
+        const uint32_t v = rows[sl].x;
+        uint32_t in = G[v];
+        while (in) {
+            const int i = __builtin_ctz(in);
+            in &= in - 1;
+            const uint32_t su = slot_of[v ^ (1u << i)];
+            if (su == 0xFFFFFFFFu) continue;  // a terminal state has no edge out of its SCC
+            // source bit i is the complement of v's
+            const uint32_t ri = 2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u);
+            emit(su >= gbeg[sl] && su < gend[sl], (su << 6) | ri);
+        }
+    };
+    for_slots([&](uint32_t a0, uint32_t a1) {
+        for (uint32_t sl = a0; sl < a1; sl++) {
+            uint32_t ci = 0, co = 0;
+            visit(sl, [&](bool inside, uint32_t) { (inside ? ci : co)++; });
+            ig_ptr[sl + 1] = ci;
+            og_ptr[sl + 1] = co;
+        }
+    });
+    for (uint32_t sl = 0; sl < M; sl++) {
+        ig_ptr[sl + 1] += ig_ptr[sl];
+        og_ptr[sl + 1] += og_ptr[sl];
     }
+    ig.resize(ig_ptr[M]);
+    og.resize(og_ptr[M]);
+    for_slots([&](uint32_t a0, uint32_t a1) {
+        for (uint32_t sl = a0; sl < a1; sl++) {
+            uint32_t pi = ig_ptr[sl], po = og_ptr[sl];
+            visit(sl, [&](bool inside, uint32_t e) {
+                if (inside)
+                    ig[pi++] = e;
+                else
+                    og[po++] = e;
+            });
+        }
+    });
+    for (SwGroup& g : P->groups) g.nin = ig_ptr[g.beg + g.ne + g.no] - ig_ptr[g.beg];
     std::vector<uint32_t> tp_ptr{0}, tp;
     for (int p = 0; p < TS; p++) {
         const uint32_t v = (uint32_t)order[p];
@@ -1112,6 +1150,9 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
         delete P;
         return rc;
     }
+    if (debug_on())
+        fprintf(stderr, "[esl-sweep] plan: %zu groups, %u slots, %.1f ms on the host\n", P->groups.size(), P->M,
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     esl_net* mnet = const_cast<esl_net*>(net);
     mnet->sweep = P;
     mnet->sweep_free = free_plan_sweep;
