@@ -149,7 +149,10 @@ def run_ours(args, rank, world, device):
     import paraexastolog_b200 as esl
 
     torch.cuda.set_device(device)
-    stream = torch.cuda.current_stream(device)
+    # one stream for torch's copies and the library's kernels, so that events on it time
+    # the library's work and copies are ordered with it
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
     ctx = esl.Context(device, stream)
     net_g, rates, x0, train_rates = workload(rank)
     model = esl.Model.parse(net_g.bnet)
@@ -190,6 +193,10 @@ def run_ours(args, rank, world, device):
 
     for _ in range(args.warmup):
         net, res = step()
+    if args.profile_run:
+        step()
+        torch.cuda.synchronize(device)
+        return None, None
     (net, res), ms, launches, clocks = timed(step, args.steps)
     iters, relres = res.report.iterations, res.report.relres
     last_xinf = res.x_inf
@@ -275,7 +282,7 @@ def run_ours(args, rank, world, device):
             "vs_baseline": None,
             "dtype": {"direct": "f64", "fp64": "f64"}.get(args.method, "f32+f64"),
             "data": "synthetic (seeded random Boolean network, log-uniform rates)",
-            "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "n_nodes": model.n,
+            "config": {"workload": f"n20_precision_network_x_{BATCH}_heldout_rate_sets", "n_nodes": model.n,
                        "states": N, "batch_rate_sets": BATCH, "initial_distributions": 1,
                        "method": "learned+mixed" if learned else args.method, "tol_relres": args.tol,
                        "l2": "working set > L2 (x_inf alone is 4 GB per step)",
@@ -340,6 +347,7 @@ def run_reference(args):
 
 
 def main():
+    global BATCH
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -353,7 +361,11 @@ def main():
                     help="skip timing the other form of the comparison (learned+mixed vs plain FP64)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=BATCH, help="held-out rate sets per step (profiling of smaller cases)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="run --warmup steps and then exactly one step, nothing else (for ncu launch lists)")
     args = ap.parse_args()
+    BATCH = args.batch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -371,6 +383,8 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     out, xinf = run_ours(args, rank, world, local)
+    if args.profile_run:
+        return
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             sample = max(8, min(os.cpu_count() or 8, 16))

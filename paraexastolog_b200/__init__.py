@@ -152,8 +152,12 @@ class Context:
         self.device = device
         torch.cuda.set_device(device)
         self.stream = stream if stream is not None else torch.cuda.current_stream(device)
+        # torch's default stream has handle 0, which the C ABI reads as "make a stream of
+        # your own"; pass cudaStreamLegacy (0x1) instead so that library work stays ordered
+        # with torch's work on that stream
+        handle = self.stream.cuda_stream or 0x1
         h = C.c_void_p()
-        check(lib().esl_ctx_create(device, C.c_void_p(self.stream.cuda_stream), C.byref(h)))
+        check(lib().esl_ctx_create(device, C.c_void_p(handle), C.byref(h)))
         self._h = h
 
     def close(self):

@@ -1553,17 +1553,22 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 // CUDA graph (one per slot parity): the small level groups are bound by the
                 // host's launch rate, not by the GPU.
                 GraphPair gp;
+                bool capturable = s != cudaStreamLegacy && s != nullptr && s != cudaStreamPerThread;
                 cudaGraph_t* graph = gp.graph;
                 cudaGraphExec_t* gexec = gp.exec;
                 int it = 0, chunk = 0;
                 for (; it < max_iters; it += kSwPoll, chunk++) {
                     const int par = chunk & 1;
-                    if (chunk == 0) {
-                        ESL_TRY(launch_chunk(par, ctx->prof));
+                    if (chunk == 0 || !capturable) {
+                        ESL_TRY(launch_chunk(par, ctx->prof && chunk == 0));
                     } else if (!gexec[par]) {
-                        int rc = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess
-                                     ? launch_chunk(par, false)
-                                     : fail(ESL_ERR_CUDA, "stream capture failed to start");
+                        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                            // the legacy default stream cannot be captured: launch directly
+                            capturable = false;
+                            ESL_TRY(launch_chunk(par, false));
+                            goto poll;
+                        }
+                        int rc = launch_chunk(par, false);
                         if (cudaStreamEndCapture(s, &graph[par]) != cudaSuccess && rc == ESL_OK)
                             rc = fail(ESL_ERR_CUDA, "stream capture failed");
                         if (rc == ESL_OK && cudaGraphInstantiate(&gexec[par], graph[par], 0) != cudaSuccess)
@@ -1576,6 +1581,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                         if (cudaGraphLaunch(gexec[par], s) != cudaSuccess)
                             return fail(ESL_ERR_CUDA, "graph launch failed");
                     }
+                poll:
                     ESL_CUDA(cudaMemcpyAsync(h_cnt + 1 + par, d_cnt + 1 + par, 4, cudaMemcpyDeviceToHost, s));
                     ESL_CUDA(cudaEventRecord(ctx->poll_ev[chunk & 1], s));
                     if (chunk >= 1) {
