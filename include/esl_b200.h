@@ -209,6 +209,8 @@ int esl_mlp_predict(esl_mlp* mlp, int B, const double* d_rates, double* d_warm);
  *      since profiling was switched on. */
 int esl_ctx_set_profiling(esl_ctx* ctx, int on);
 int esl_ctx_profile(esl_ctx* ctx, double* total_ms, double* total_bytes, int* launches);
+/* the same per recorded application: *count records, the first `cap` written */
+int esl_ctx_profile_records(esl_ctx* ctx, int cap, double* ms, double* bytes, int* count);
 /* number of kernels this library has launched in this process (no counterpart in the reference) */
 int esl_launch_count(uint64_t* count);
 

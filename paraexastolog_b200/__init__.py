@@ -71,6 +71,7 @@ def lib():
     L.esl_ctx_set_profiling.argtypes = [vp, C.c_int]
     L.esl_launch_count.argtypes = [P(C.c_uint64)]
     L.esl_ctx_profile.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_int)]
+    L.esl_ctx_profile_records.argtypes = [vp, C.c_int, vp, vp, P(C.c_int)]
     L.esl_model_load.argtypes = [cp, P(vp)]
     L.esl_model_parse.argtypes = [cp, P(vp)]
     L.esl_model_free.argtypes = [vp]
@@ -183,6 +184,16 @@ class Context:
         ms, by, n = C.c_double(), C.c_double(), C.c_int()
         check(lib().esl_ctx_profile(self._h, C.byref(ms), C.byref(by), C.byref(n)))
         return ms.value, by.value, n.value
+
+    def profile_records(self):
+        """Per recorded operator application: (device ms, algorithmic bytes) arrays."""
+        n = C.c_int()
+        check(lib().esl_ctx_profile_records(self._h, 0, None, None, C.byref(n)))
+        ms = np.zeros(n.value)
+        by = np.zeros(n.value)
+        if n.value:
+            check(lib().esl_ctx_profile_records(self._h, n.value, _ptr(ms), _ptr(by), C.byref(n)))
+        return ms, by
 
 
 class Model:

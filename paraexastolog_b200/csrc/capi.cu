@@ -165,6 +165,19 @@ int esl_ctx_profile(esl_ctx* c, double* total_ms, double* total_bytes, int* laun
     return ESL_OK;
 }
 
+int esl_ctx_profile_records(esl_ctx* c, int cap, double* ms, double* bytes, int* count) {
+    if (!c || !count || cap < 0 || (cap > 0 && (!ms || !bytes))) return fail(ESL_ERR_INVALID, "bad argument");
+    ESL_CUDA(cudaStreamSynchronize(c->stream));
+    *count = (int)c->prof_recs.size();
+    for (int i = 0; i < cap && i < *count; i++) {
+        float t = 0.f;
+        ESL_CUDA(cudaEventElapsedTime(&t, c->prof_recs[i].a, c->prof_recs[i].b));
+        ms[i] = t;
+        bytes[i] = c->prof_recs[i].bytes;
+    }
+    return ESL_OK;
+}
+
 int esl_ctx_synchronize(esl_ctx* c) {
     if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
     ESL_CUDA(cudaStreamSynchronize(c->stream));
