@@ -160,6 +160,25 @@ int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rat
                     const double* d_x0, double* d_x_inf, double* d_marginals,
                     const esl_solve_opts* opts, esl_report* report);
 
+/* ---- many networks in one call.  No counterpart in the reference, which solves one
+ *      network per run (cuda/src/main.cpp:102-157).  Each job is one esl_solve_batch;
+ *      the contexts of the pool (each with its own stream and workspace; create them on
+ *      one device or several) run the jobs concurrently from host threads, largest
+ *      first, so that small networks overlap on the GPU.  Returns the first failing
+ *      job's status; every job's status and report are written back. */
+typedef struct esl_job {
+    const esl_net* net;
+    int B;                   /* rate sets (d_rates B x 2n, same zero pattern as net) */
+    const double* d_rates;
+    int R;                   /* initial distributions (d_x0 R x N) */
+    const double* d_x0;
+    double* d_x_inf;         /* B x R x N */
+    double* d_marginals;     /* B x R x n, or NULL */
+    esl_report report;       /* out */
+    int status;              /* out */
+} esl_job;
+int esl_solve_many(esl_ctx* const* ctxs, int n_ctx, esl_job* jobs, int n_jobs, const esl_solve_opts* opts);
+
 /* Host-memory end-to-end call: bnet text, rates (B x 2n) and x0 (R x N) on the host,
  * results copied back to host buffers.  Builds and frees its own net. */
 int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,

@@ -49,6 +49,11 @@ class Report(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("relres", C.c_double), ("converged", C.c_int)]
 
 
+class Job(C.Structure):
+    _fields_ = [("net", C.c_void_p), ("B", C.c_int), ("d_rates", C.c_void_p), ("R", C.c_int), ("d_x0", C.c_void_p),
+                ("d_x_inf", C.c_void_p), ("d_marginals", C.c_void_p), ("report", Report), ("status", C.c_int)]
+
+
 def header_functions() -> list:
     """Names of the functions declared in include/esl_b200.h."""
     text = open(HEADER).read()
@@ -96,6 +101,7 @@ def lib():
     L.esl_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_batch.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_host.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
+    L.esl_solve_many.argtypes = [vp, C.c_int, P(Job), C.c_int, P(SolveOpts)]
     f32 = C.c_float
     L.esl_mlp_create.argtypes = [vp, vp, C.c_uint64, P(vp)]
     L.esl_mlp_free.argtypes = [vp]
@@ -447,6 +453,7 @@ class SolveResult:
     R: object = None
     L: object = None
     report: Optional[Report] = None
+    status: int = 0
 
 
 def _opts(method: int, tol: float, max_iters: int, max_refine: int, warm=None, occupation=None) -> SolveOpts:
@@ -496,6 +503,39 @@ def solve_batch(ctx: Context, net: Net, rates, x0, method: int = METHOD_FP64, to
     check(lib().esl_solve_batch(ctx._h, net._h, B, _ptr(rates), R, _ptr(x0), _ptr(xi), _ptr(mg), C.byref(o),
                                 C.byref(rep)))
     return SolveResult(xi, mg, report=rep)
+
+
+def solve_many(ctxs: Sequence[Context], jobs, method: int = METHOD_DIRECT, tol: float = 1e-10,
+               max_iters: int = 0, max_refine: int = 0, raise_on_error: bool = True):
+    """Many (net, rates B x 2n, x0 R x N) jobs in one call, run concurrently over the
+    contexts (give each its own stream); returns one SolveResult per job (with its
+    status; the first failure raises unless raise_on_error is False)."""
+    torch = _torch()
+    keep, arr = [], (Job * max(1, len(jobs)))()
+    results = []
+    for i, (net, rates, x0) in enumerate(jobs):
+        dev = f"cuda:{net.ctx.device}"
+        r = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
+        x = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
+        r = r[None] if r.dim() == 1 else r
+        x = x[None] if x.dim() == 1 else x
+        B, R = r.shape[0], x.shape[0]
+        xi = torch.empty((B, R, net.N), dtype=torch.float64, device=dev)
+        mg = torch.empty((B, R, net.n), dtype=torch.float64, device=dev)
+        keep += [r, x]
+        arr[i] = Job(net._h.value if hasattr(net._h, "value") else net._h, B, _ptr(r), R, _ptr(x), _ptr(xi), _ptr(mg),
+                     Report(), 0)
+        results.append(SolveResult(xi, mg))
+    handles = (C.c_void_p * len(ctxs))(*[c._h.value if hasattr(c._h, "value") else c._h for c in ctxs])
+    torch.cuda.synchronize()
+    o = _opts(method, tol, max_iters, max_refine)
+    rc = lib().esl_solve_many(C.cast(handles, C.c_void_p), len(ctxs), arr, len(jobs), C.byref(o))
+    for i, res in enumerate(results):
+        res.report = arr[i].report
+        res.status = arr[i].status
+    if raise_on_error:
+        check(rc)
+    return results
 
 
 def solve_host(ctx: Context, model: Model, rates: np.ndarray, x0: np.ndarray, method: int = METHOD_FP64,

@@ -14,7 +14,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libesl_b200.so")
-SOURCES = ["capi.cu", "table.cu", "table_static.cu", "graph.cu", "solve.cu", "sweep.cu", "mlp.cu", "model.cpp"]
+SOURCES = ["capi.cu", "table.cu", "table_static.cu", "graph.cu", "solve.cu", "sweep.cu", "mlp.cu", "multi.cu", "model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

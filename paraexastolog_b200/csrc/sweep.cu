@@ -1233,6 +1233,12 @@ bool debug_on() {
 
 void free_sweep_workspace(void* w) { delete static_cast<Workspace*>(w); }
 
+int sweep_prepare(esl_ctx* ctx, const esl_net* net) {
+    if (!sweep_supported(net)) return ESL_OK;
+    SweepPlan* P = nullptr;
+    return build_plan(ctx, net, P);
+}
+
 int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& states) {
     if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
     SweepPlan* P = nullptr;
