@@ -14,6 +14,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libesl_b200.so")
+CLI = os.path.join(OUT_DIR, "esl_cli")
 SOURCES = ["capi.cu", "table.cu", "table_static.cu", "graph.cu", "solve.cu", "sweep.cu", "mlp.cu", "multi.cu", "model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,6 +51,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
         subprocess.run(cmd, check=True)
     if force or not _newer(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    # the reference's command line over the C ABI
+    cli_src = os.path.join(CSRC, "cli.cpp")
+    if force or not _newer(CLI, [cli_src, LIB] + headers):
+        cmd = [nvcc()] + ARCH + ["-O2", "-std=c++17", "-I" + os.path.join(REPO, "include"), cli_src, "-o", CLI,
+               "-L" + OUT_DIR, "-lesl_b200", "-lcudart", "-Xlinker", "-rpath=$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -1545,6 +1545,65 @@ int make_layout(esl_ctx* ctx, Workspace& ws, const esl_net* net, int dom, const 
 
 }  // namespace
 
+// L (T x N) from forward solves: column s of L is the mass that each terminal SCC receives
+// from a unit initial distribution at transient state s (the level sweep's terminal
+// masses), solved for chunks of transient states at a time.  Terminal columns are
+// L[t][v] = [v in t].  The fallback of the backward form.
+__global__ void k_unit_rows(int c, size_t N, const int32_t* __restrict__ order, int64_t first,
+                            double* __restrict__ x0) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < c) x0[(size_t)j * N + order[first + j]] = 1.0;
+}
+
+__global__ void k_L_columns(int c, int T, size_t N, const int32_t* __restrict__ order, int64_t first,
+                            const double* __restrict__ y, double* __restrict__ Lm) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= c) return;
+    const size_t v = (size_t)order[first + j];
+    for (int t = 0; t < T; t++) Lm[(size_t)t * N + v] = y[(size_t)j * T + t];
+}
+
+__global__ void k_L_terminals(size_t N, int T, const int32_t* __restrict__ term_of, double* __restrict__ Lm) {
+    const size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N || term_of[v] < 0) return;
+    for (int t = 0; t < T; t++) Lm[(size_t)t * N + v] = term_of[v] == t ? 1.0 : 0.0;
+}
+
+int absorption_by_sweep(esl_ctx* ctx, Workspace& ws, const esl_net* net, const double* d_rates,
+                        const esl_solve_opts& o, double* d_L) {
+    cudaStream_t s = ctx->stream;
+    const size_t N = (size_t)net->N;
+    const int T = net->T;
+    const int64_t TS = net->term_states, M = (int64_t)N - TS;
+    // unit initial distributions of up to ~1 GB per chunk
+    const int chunk = (int)std::max<int64_t>(32, std::min<int64_t>(4096, (int64_t)((1ull << 30) / (8 * N))));
+    int st_ = ESL_OK;
+    double* x0 = (double*)ws.get(S_XSUB, (size_t)chunk * N * 8, &st_);
+    double* y = (double*)ws.get(S_SUM, (size_t)chunk * T * 8, &st_);
+    if (st_ != ESL_OK) return st_;
+    esl_solve_opts so = o;
+    so.method = ESL_METHOD_DIRECT;
+    so.d_warm = nullptr;
+    so.d_occupation = nullptr;
+    ESL_CUDA(cudaMemsetAsync(d_L, 0, (size_t)T * N * 8, s));
+    for (int64_t first = 0; first < M; first += chunk) {
+        const int c = (int)std::min<int64_t>(chunk, M - first);
+        ESL_CUDA(cudaMemsetAsync(x0, 0, (size_t)c * N * 8, s));
+        ESL_COUNT_LAUNCH();
+        k_unit_rows<<<(c + 127) / 128, 128, 0, s>>>(c, N, net->order.get(), TS + first, x0);
+        ESL_CUDA(cudaMemsetAsync(y, 0, (size_t)c * T * 8, s));
+        SweepStats sw;
+        ESL_TRY(sweep_forward(ctx, net, c, c, d_rates, x0, N, so, y, sw));
+        ESL_COUNT_LAUNCH();
+        k_L_columns<<<(c + 127) / 128, 128, 0, s>>>(c, T, N, net->order.get(), TS + first, y, d_L);
+        ESL_CUDA(cudaGetLastError());
+    }
+    ESL_COUNT_LAUNCH();
+    k_L_terminals<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(N, T, net->term_of.get(), d_L);
+    ESL_CUDA(cudaGetLastError());
+    return ESL_OK;
+}
+
 int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                 double* d_x_inf, double* d_marg, double* d_R, double* d_L, const esl_solve_opts* opts,
                 esl_report* rep) {
@@ -1847,11 +1906,19 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             SolveOut so;
             esl_solve_opts lo = o;
             lo.d_warm = nullptr;
+            lo.d_occupation = nullptr;
             lo.max_iters = std::max(o.max_iters, 5000);
-            ESL_TRY(krylov_solve<false>(ctx, ws, L, d_rates, T, bE, bO, nullptr, 0, lo, x64, zE, so));
-            ESL_COUNT_LAUNCH();
-            k_scatter_L<<<g, kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), zE, x64, d_L);
-            ESL_CUDA(cudaGetLastError());
+            const int rc = krylov_solve<false>(ctx, ws, L, d_rates, T, bE, bO, nullptr, 0, lo, x64, zE, so);
+            if (rc == ESL_OK) {
+                ESL_COUNT_LAUNCH();
+                k_scatter_L<<<g, kT, 0, s>>>(L.H, T, N, L.ld, net->term_of.get(), zE, x64, d_L);
+                ESL_CUDA(cudaGetLastError());
+            } else if (rc == ESL_ERR_NOT_CONVERGED && sweep_supported(net)) {
+                if (debug_enabled()) fprintf(stderr, "[esl] L: backward solve missed its tolerance, forward sweep\n");
+                ESL_TRY(absorption_by_sweep(ctx, ws, net, d_rates, o, d_L));
+            } else {
+                return rc;
+            }
         } else {
             // every state terminal: L[t][v] = [v in t]
             ESL_CUDA(cudaMemsetAsync(d_L, 0, (size_t)T * N * 8, s));

@@ -266,3 +266,17 @@ def test_host_api_matches_device_api(esl, ctx):
     ox, omarg = om.analyse(w.rates[0][0]).solve(w.x0[0][0])
     assert np.abs(xi[0, 0] - ox).sum() <= 1e-9
     assert rep.converged == 1
+
+
+@pytest.mark.parametrize("method", [0, 2])
+def test_absorption_matrix_kras(esl, ctx, goldens, method):
+    # 40 terminal SCCs; L is checked against the oracle's absorption probabilities
+    text = goldens["models"]["krasmodel15vars.bnet"]
+    m = esl.Model.parse(text)
+    r = m.rates_uniform()
+    net = esl.Net.build(ctx, m, r)
+    x0 = m.initial_state(ctx)
+    res = esl.solve(ctx, net, r, x0, want_L=True, method=method)
+    Lo = O.Model(text=text).analyse(r).absorption(r)
+    L = res.L.cpu().numpy()
+    assert np.abs(L - Lo.reshape(L.shape)).max() <= 1e-9
