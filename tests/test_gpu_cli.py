@@ -67,7 +67,8 @@ def _run(cli, path, *args):
     return p.stdout
 
 
-@pytest.mark.parametrize("name", ["solver.toy", "solver.kras", "rates.toy", "zero_rate.toy", "solver.mammal"])
+@pytest.mark.parametrize("name", ["solver.toy", "solver.kras", "rates.toy", "zero_rate.toy", "solver.mammal",
+                                  "solver.zanudo"])
 def test_cli_goldens(esl, cli, goldens, tmp_path, name):
     c = goldens["cases"][name]
     text = goldens["models"][c["model"]]

@@ -280,3 +280,40 @@ def test_absorption_matrix_kras(esl, ctx, goldens, method):
     Lo = O.Model(text=text).analyse(r).absorption(r)
     L = res.L.cpu().numpy()
     assert np.abs(L - Lo.reshape(L.shape)).max() <= 1e-9
+
+
+WIDE_AND_CONSTANT = ("targets, factors\nA, B & C & D & E & F & !G\nB, 1\nC, 0\nD, A | B\nE, !E\n"
+                     "F, (A & !B) | (C & D) | (E & G)\nG, A\nH, true\nI, FALSE & H\n")
+
+
+def test_constants_and_six_input_rules(esl, ctx):
+    # rules over 6 inputs and constant rules (1, 0, true, FALSE)
+    om = O.Model(text=WIDE_AND_CONSTANT)
+    m = esl.Model.parse(WIDE_AND_CONSTANT)
+    r = _rates(m.n, 8)
+    ip, rows, cols = esl.table(ctx, m, r)
+    rip, rrows, rcols = om.table(r)
+    assert np.array_equal(ip.cpu().numpy(), rip) and np.array_equal(rows.cpu().numpy(), rrows)
+    assert np.array_equal(cols.cpu().numpy(), rcols)
+    net = esl.Net.build(ctx, m, r)
+    x0 = np.full(1 << m.n, 1.0 / (1 << m.n))
+    res = esl.solve(ctx, net, r, x0, method=esl.METHOD_DIRECT, tol=1e-12)
+    ox, om_marg = om.analyse(r).solve(x0)
+    assert np.abs(res.x_inf.cpu().numpy() - ox).sum() <= 1e-9
+
+
+def test_zanudo_golden_n23(esl, ctx, goldens):
+    # the reference's largest known-answer case: 23 nodes, 8,388,608 states
+    c = goldens["cases"]["solver.zanudo"]
+    m = esl.Model.parse(goldens["models"][c["model"]])
+    assert m.n == 23
+    r = m.rates_uniform()
+    net = esl.Net.build(ctx, m, r)
+    x0 = m.initial_state(ctx, c["fixed"], c["values"])
+    res = esl.solve(ctx, net, r, x0, method=esl.METHOD_DIRECT, tol=1e-12)
+    xi = res.x_inf.cpu().numpy()
+    idx, val = nonzeros(xi)
+    big = idx[val > 1e-12]
+    assert big.tolist() == c["nonzero_indices"]
+    np.testing.assert_allclose(xi[big], c["nonzero_data"], atol=128 * FLT_EPS, rtol=0)
+    assert abs(xi.sum() - 1.0) <= 1e-12
