@@ -56,7 +56,7 @@ constexpr int SW_IDONE = 8;  // its inner solve has stopped
 
 // per-system scalar arrays (doubles), each Kp long
 enum Scal { C_BB, C_RR64, C_PREV, C_RHO, C_R0V, C_TS, C_TT, C_RR, C_RN, C_BETA, C_OMEGA, C_TARGET, C_BEST, C_SCALE,
-            C_NSCAL };
+            C_R0T, C_NSCAL };
 // per-system int arrays
 enum IScal { I_FLAGS, I_ITERS, I_NOIMP, I_TOTAL, I_STALL, I_NISCAL };
 
@@ -332,22 +332,25 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
 //   MODE 2: Y = y                        acc0 += AUX . Y   (AUX = r0)
 //   MODE 3: Y = y                        acc0 += Y . (AUX X), acc1 += Y . Y   (AUX = dS)
 //   MODE 4: (no output)                  acc0 += y . B, acc1 += y . y   (B = reduced rhs)
+//   MODE 6: as MODE 3, and acc2 += R0x . Y (so that the next beta is known before the
+//           x / r update: beta = -(r0 . t) / (r0 . v))
 // S systems per thread.  X, AUX and Y are streamed (evict-first) so that the gathered W
 // keeps its place in L2.
 template <int S, int MODE, class T>
 __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict__ X, const T* __restrict__ W,
                                                    const double* __restrict__ B, const T* __restrict__ AUX,
-                                                   T* __restrict__ Y, double* acc0, double* acc1) {
+                                                   T* __restrict__ Y, double* acc0, double* acc1,
+                                                   const T* __restrict__ R0x, double* acc2) {
     extern __shared__ unsigned char s_raw[];
     T* s_rate = reinterpret_cast<T*>(s_raw);
     const Tile t = tile_of<S>(a.KT);
     sw_rates(s_rate, a, t);
-    double d0[S], d1[S];
+    double d0[S], d1[S], d2[S];
     bool act[S];
     bool any = false;
 #pragma unroll
     for (int q = 0; q < S; q++) {
-        d0[q] = d1[q] = 0.0;
+        d0[q] = d1[q] = d2[q] = 0.0;
         const int k = t.k + q * t.TR;
         act[q] = !((MODE >= 2) ? sw_skip(a, k) : (k >= a.K));
         any |= act[q];
@@ -389,12 +392,23 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
                         __stcs(Y + i, y);
                         d0[q] += (double)y * ((double)__ldcs(AUX + i) * (double)x);
                         d1[q] += (double)y * (double)y;
+                        if (MODE == 6) d2[q] += (double)__ldcs(R0x + i) * (double)y;
                     }
                 }
             }
         }
     }
-    if (MODE == 3 || MODE == 4) {
+    if (MODE == 6) {
+        double v[3][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) {
+            v[0][q] = d0[q];
+            v[1][q] = d1[q];
+            v[2][q] = d2[q];
+        }
+        double* const dst[3] = {acc0, acc1, acc2};
+        sw_reduce<3, S>(v, dst, t, a.K);
+    } else if (MODE == 3 || MODE == 4) {
         double v[2][S];
 #pragma unroll
         for (int q = 0; q < S; q++) {
@@ -419,19 +433,6 @@ struct SwScalPtr {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kSwT) k_sw_p(SwArgs a, SwScalPtr sc, const T* __restrict__ R, const T* __restrict__ dS,
-                                               const T* __restrict__ V, T* __restrict__ PH) {
-    const Tile t = tile_of(a.KT);
-    if (sw_skip(a, t.k)) return;
-    const T beta = (T)sc.c[C_BETA][t.k], omega = (T)sc.c[C_OMEGA][t.k];
-    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
-        const size_t idx = (size_t)r * a.Kp + t.k;
-        const T d = dS[idx];
-        PH[idx] = (R[idx] + beta * (d * PH[idx] - omega * V[idx])) / d;
-    }
-}
-
-template <class T>
 __global__ void __launch_bounds__(kSwT) k_sw_s(SwArgs a, SwScalPtr sc, const T* __restrict__ R, const T* __restrict__ V,
                                                const T* __restrict__ dS, T* __restrict__ SH) {
     const Tile t = tile_of(a.KT);
@@ -444,23 +445,29 @@ __global__ void __launch_bounds__(kSwT) k_sw_s(SwArgs a, SwScalPtr sc, const T* 
     }
 }
 
+// x / r update fused with the next search direction.  With alpha = rho / (r0 . v),
+// omega = (t . s) / (t . t) and, from r0 . s = 0, beta = -(r0 . t) / (r0 . v):
+//   D += alpha PH + omega SH,  R = s - omega t,  PH = (R + beta (dS PH - omega V)) / dS.
+// A system that stops at this iteration gets a direction it never uses.
 template <class T>
-__global__ void __launch_bounds__(kSwT) k_sw_xr(SwArgs a, SwScalPtr sc, const T* __restrict__ PH,
-                                                const T* __restrict__ SH, const T* __restrict__ dS,
-                                                const T* __restrict__ TT, const T* __restrict__ R0, T* __restrict__ D,
-                                                T* __restrict__ R) {
+__global__ void __launch_bounds__(kSwT) k_sw_xrp(SwArgs a, SwScalPtr sc, T* __restrict__ PH,
+                                                 const T* __restrict__ SH, const T* __restrict__ dS,
+                                                 const T* __restrict__ TT, const T* __restrict__ R0,
+                                                 const T* __restrict__ V, T* __restrict__ D, T* __restrict__ R) {
     const Tile t = tile_of(a.KT);
     double d0 = 0.0, d1 = 0.0;
     if (!sw_skip(a, t.k)) {
         const double r0v = sc.c[C_R0V][t.k], tt = sc.c[C_TT][t.k];
         const T alpha = r0v != 0.0 ? (T)(sc.c[C_RHO][t.k] / r0v) : (T)0;
         const T omega = tt > 0.0 ? (T)(sc.c[C_TS][t.k] / tt) : (T)0;
+        const T beta = r0v != 0.0 ? (T)(-sc.c[C_R0T][t.k] / r0v) : (T)0;
         for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
             const size_t idx = (size_t)r * a.Kp + t.k;
-            const T sh = __ldcs(SH + idx);
-            __stcs(D + idx, __ldcs(D + idx) + alpha * __ldcs(PH + idx) + omega * sh);
-            const T rn = __ldcs(dS + idx) * sh - omega * __ldcs(TT + idx);
+            const T sh = __ldcs(SH + idx), ph = PH[idx], d = __ldcs(dS + idx);
+            __stcs(D + idx, __ldcs(D + idx) + alpha * ph + omega * sh);
+            const T rn = d * sh - omega * __ldcs(TT + idx);
             __stcs(R + idx, rn);
+            PH[idx] = (rn + beta * (d * ph - omega * __ldcs(V + idx))) / d;
             d0 += (double)rn * (double)rn;
             d1 += (double)__ldcs(R0 + idx) * (double)rn;
         }
@@ -501,7 +508,7 @@ __global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int* active) {
             sc.c[C_RHO][k] = rn;
             cnt++;
         }
-        sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = 0.0;
+        sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = sc.c[C_R0T][k] = 0.0;
     }
     atomicAdd(&s_cnt, cnt);
     __syncthreads();
@@ -540,7 +547,7 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
         sc.c[C_TARGET][k] = fmax(inner_rel2, 0.01 * tol2 * b2 * scale * scale);
         sc.c[C_BEST][k] = 1.0;
         sc.i[I_STALL][k] = 0;
-        sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = 0.0;
+        sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = sc.c[C_R0T][k] = 0.0;
         cnt++;
     }
     atomicAdd(&s_cnt, cnt);
@@ -548,12 +555,13 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
     if (threadIdx.x == 0) *active = s_cnt;
 }
 
-// start of an inner solve: R = R0 = (T) (R64 * scale), D = PH = V = 0
+// start of an inner solve: R = R0 = (T) (R64 * scale), PH = R / dS (the first search
+// direction), D = V = 0
 template <class T>
 __global__ void __launch_bounds__(kSwT) k_sw_start(SwArgs a, const double* __restrict__ scale,
-                                                   const double* __restrict__ R64, T* __restrict__ R,
-                                                   T* __restrict__ R0, T* __restrict__ D, T* __restrict__ PH,
-                                                   T* __restrict__ V) {
+                                                   const double* __restrict__ R64, const T* __restrict__ dS,
+                                                   T* __restrict__ R, T* __restrict__ R0, T* __restrict__ D,
+                                                   T* __restrict__ PH, T* __restrict__ V) {
     const Tile t = tile_of(a.KT);
     if (sw_skip(a, t.k)) return;
     const double sk = scale[t.k];
@@ -563,7 +571,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_start(SwArgs a, const double* __res
         R[idx] = x;
         R0[idx] = x;
         D[idx] = 0;
-        PH[idx] = 0;
+        PH[idx] = x / dS[idx];
         V[idx] = 0;
     }
 }
@@ -1160,7 +1168,8 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     return ESL_OK;
 }
 
-// systems per CTA tile: a divisor of Kp, at most 128, and rates of the tile within 40 KB.
+// systems per CTA tile: a divisor of Kp, at most 128, and rates of the tile within 36 KB
+// (with the reduction arrays the kernels stay inside the default 48 KB of shared memory).
 // With `rows` > 0 the tile is also narrowed (down to 32) until one tile's slice of a
 // vector over `rows` rows fits in the slice budget, so that the neighbour gathers of a
 // Krylov iteration hit L2.  The budget is a tuning parameter (ESL_SWEEP_TILE_MB,
@@ -1189,7 +1198,7 @@ double mixed_inner_rel() {
 
 int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0) {
     int kt = 128;
-    while (kt > 32 && (Kp % kt != 0 || (size_t)2 * n * kt * elem > 40 * 1024 ||
+    while (kt > 32 && (Kp % kt != 0 || (size_t)2 * n * kt * elem > 36 * 1024 ||
                        (size_t)rows * kt * elem > tile_bytes()))
         kt >>= 1;
     return kt;
@@ -1375,7 +1384,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, (const double*)nullptr, W64);
         ESL_COUNT_LAUNCH();
         k_sw_apply<1, 0, double><<<go, kSwT, gsm64, s>>>(a, nullptr, W64, Bv + (size_t)g.ne * Kp, nullptr, bS,
-                                                     sc.c[C_BB], nullptr);
+                                                     sc.c[C_BB], nullptr, nullptr, nullptr);
         ESL_COUNT_LAUNCH();
         k_sw_init<<<go, kSwT, 0, s>>>(a, o.d_warm, (size_t)net->N, bS, dS64, X64);
         ESL_CUDA(cudaGetLastError());
@@ -1452,7 +1461,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             ESL_COUNT_LAUNCH();
             k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
             ESL_COUNT_LAUNCH();
-            k_sw_apply<1, 1, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, R64, sc.c[C_RR64], nullptr);
+            k_sw_apply<1, 1, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, R64, sc.c[C_RR64], nullptr, nullptr, nullptr);
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         };
@@ -1464,7 +1473,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
             ESL_COUNT_LAUNCH();
             k_sw_apply<1, 4, double><<<go, kSwT, gsm64, s>>>(a, X64, W64, bS, nullptr, nullptr, sc.c[C_R0V],
-                                                              sc.c[C_TS]);
+                                                              sc.c[C_TS], nullptr, nullptr);
             ESL_COUNT_LAUNCH();
             k_sw_warm_scale<<<go, kSwT, 0, s>>>(a, sc.c[C_R0V], sc.c[C_TS], X64);
             ESL_CUDA(cudaGetLastError());
@@ -1506,12 +1515,10 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 const double op_bytes = (double)nrun * sizeof(TT) * (4.0 * g.no + 2.0 * g.ne) +
                                         12.0 * (g.ne + g.no) + 4.0 * (double)g.nin;
                 ESL_COUNT_LAUNCH();
-                k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, R, R0, D, PH, V);
+                k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, dS, R, R0, D, PH, V);
                 // kSwPoll iterations; `par` picks the running-count slot of this poll window
                 auto launch_chunk = [&](int par, bool record) -> int {
                     for (int j = 0; j < kSwPoll; j++) {
-                    ESL_COUNT_LAUNCH();
-                    k_sw_p<TT><<<goi, kSwT, 0, s>>>(a, sc, R, dS, V, PH);
                     const bool rec = record;
                     cudaEvent_t ea = nullptr, eb = nullptr;
                     if (rec) {
@@ -1526,9 +1533,9 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                         k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
                     ESL_COUNT_LAUNCH();
                     if (s2)
-                        k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                        k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
                     else
-                        k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr);
+                        k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
                     if (rec) {
                         ESL_CUDA(cudaEventRecord(eb, s));
                         ctx->prof_recs.push_back({ea, eb, op_bytes});
@@ -1542,13 +1549,13 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                         k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
                     ESL_COUNT_LAUNCH();
                     if (s2)
-                        k_sw_apply<2, 3, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                      sc.c[C_TT]);
+                        k_sw_apply<2, 6, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                      sc.c[C_TT], R0, sc.c[C_R0T]);
                     else
-                        k_sw_apply<1, 3, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                      sc.c[C_TT]);
+                        k_sw_apply<1, 6, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                      sc.c[C_TT], R0, sc.c[C_R0T]);
                     ESL_COUNT_LAUNCH();
-                    k_sw_xr<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, D, R);
+                    k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                     ESL_COUNT_LAUNCH();
                     k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, d_cnt + 1 + par);
                     }
@@ -1583,7 +1590,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                             rc = fail(ESL_ERR_CUDA, "graph launch failed");
                         if (rc != ESL_OK) return rc;
                     } else {
-                        count_launches(8 * kSwPoll);
+                        count_launches(7 * kSwPoll);
                         if (cudaGraphLaunch(gexec[par], s) != cudaSuccess)
                             return fail(ESL_ERR_CUDA, "graph launch failed");
                     }
