@@ -191,6 +191,10 @@ def run_ours(args, rank, world, device):
             barrier()
         return out, e0.elapsed_time(e1), esl.launch_count() - l0, clk.summary()
 
+    tuning = None
+    if not args.no_autotune and not args.profile_run:
+        # level-sweep tiling for this batch, picked by timing (outside the timed region)
+        tuning = esl.Net.build(ctx, model, rates[0]).autotune(d_rates, d_x0, method=solve_method, tol=args.tol)
     for _ in range(args.warmup):
         net, res = step()
     if args.profile_run:
@@ -314,6 +318,8 @@ def run_ours(args, rank, world, device):
             "solver": {"iterations": iters, "relres": relres},
             "clocks": clocks,
         }
+        if tuning:
+            out["config"]["tiling"] = tuning
         if other:
             other["value_over_headline"] = other["value"] / value
             out["learned_mixed" if other["method"] == "learned+mixed" else "plain_fp64"] = other
@@ -372,6 +378,7 @@ def main():
                     help="skip timing the other form of the comparison (learned+mixed vs plain FP64)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default level-sweep tiling")
     ap.add_argument("--batch", type=int, default=BATCH, help="held-out rate sets per step (profiling of smaller cases)")
     ap.add_argument("--profile-run", action="store_true",
                     help="run --warmup steps and then exactly one step, nothing else (for ncu launch lists)")

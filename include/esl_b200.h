@@ -143,6 +143,13 @@ int esl_net_info(const esl_net* net, int* n_nodes, int* n_sccs, int* n_terminals
  * (min vertex of the SCC).  Any pointer may be NULL. */
 int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* d_offsets,
                    int32_t* d_levels, int32_t* d_labels);
+/* Autotuner (no counterpart in the reference): times the batch solve of the level sweep
+ * under a few tilings (the L2 slice budget that sets the systems per tile, and one or two
+ * systems per thread in the gather kernels), keeps the fastest in `net` (and in `ctx`, for
+ * networks built later on it) and returns it.  Run it outside any timed region; it solves
+ * the batch five times. */
+int esl_net_autotune(esl_ctx* ctx, esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
+                     const esl_solve_opts* opts, int* tile_mb, int* two_per_thread, double* ms);
 /* 1 if the rate set has the zero pattern the net was built for */
 int esl_net_compatible(const esl_net* net, const double* rates, int* compatible);
 

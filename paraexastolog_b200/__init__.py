@@ -98,6 +98,8 @@ def lib():
     L.esl_net_info.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_int)]
     L.esl_net_export.argtypes = [vp, vp, vp, vp, vp, vp]
     L.esl_net_compatible.argtypes = [vp, vp, P(C.c_int)]
+    L.esl_net_autotune.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, P(SolveOpts), P(C.c_int), P(C.c_int),
+                                   P(C.c_double)]
     L.esl_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_batch.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
     L.esl_solve_host.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, P(SolveOpts), P(Report)]
@@ -327,6 +329,20 @@ class Net:
         labels = torch.empty(self.N, dtype=torch.int32, device=dev)
         check(lib().esl_net_export(self.ctx._h, self._h, _ptr(order), _ptr(offsets), _ptr(levels), _ptr(labels)))
         return order, offsets, levels[: self.n_sccs], labels
+
+    def autotune(self, rates, x0, method: int = METHOD_DIRECT, tol: float = 1e-10) -> dict:
+        """Time the batch solve under a few level-sweep tilings and keep the fastest."""
+        torch = _torch()
+        dev = f"cuda:{self.ctx.device}"
+        r = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
+        x = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
+        r = r[None] if r.dim() == 1 else r
+        x = x[None] if x.dim() == 1 else x
+        mb, s2, ms = C.c_int(), C.c_int(), C.c_double()
+        o = _opts(method, tol, 0, 0)
+        check(lib().esl_net_autotune(self.ctx._h, self._h, r.shape[0], _ptr(r), x.shape[0], _ptr(x), C.byref(o),
+                                     C.byref(mb), C.byref(s2), C.byref(ms)))
+        return {"tile_mb": mb.value, "two_systems_per_thread": bool(s2.value), "ms": ms.value}
 
     def compatible(self, rates: np.ndarray) -> bool:
         rates = np.ascontiguousarray(rates, np.float64)

@@ -178,6 +178,55 @@ int esl_ctx_profile_records(esl_ctx* c, int cap, double* ms, double* bytes, int*
     return ESL_OK;
 }
 
+int esl_net_autotune(esl_ctx* c, esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
+                     const esl_solve_opts* opts, int* tile_mb, int* two_per_thread, double* ms_out) {
+    if (!c || !net || !d_rates || !d_x0 || B < 1 || R < 1) return fail(ESL_ERR_INVALID, "bad argument");
+    const size_t N = (size_t)net->N;
+    double *xi = nullptr;
+    if (cudaMalloc(&xi, (size_t)B * R * N * 8) != cudaSuccess) return fail(ESL_ERR_NOMEM, "autotune buffer");
+    struct Cand {
+        int mb, s2;
+    };
+    const Cand cands[] = {{48, 1}, {48, 0}, {16, 1}, {128, 1}};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = -1, rc = ESL_OK;
+    float best_ms = 0.f;
+    // one untimed solve first, so that the plan and workspaces exist
+    net->tune_tile_mb = cands[0].mb;
+    net->tune_s2 = cands[0].s2;
+    rc = esl_solve_batch(c, net, B, d_rates, R, d_x0, xi, nullptr, opts, nullptr);
+    for (int i = 0; rc == ESL_OK && i < (int)(sizeof cands / sizeof cands[0]); i++) {
+        net->tune_tile_mb = cands[i].mb;
+        net->tune_s2 = cands[i].s2;
+        cudaEventRecord(e0, c->stream);
+        rc = esl_solve_batch(c, net, B, d_rates, R, d_x0, xi, nullptr, opts, nullptr);
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rc == ESL_OK && (best < 0 || ms < best_ms)) {
+            best = i;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(xi);
+    if (best < 0) {
+        net->tune_tile_mb = 0;
+        net->tune_s2 = -1;
+        return rc != ESL_OK ? rc : fail(ESL_ERR_INVALID, "autotune found no configuration");
+    }
+    net->tune_tile_mb = c->tune_tile_mb = cands[best].mb;
+    net->tune_s2 = c->tune_s2 = cands[best].s2;
+    if (tile_mb) *tile_mb = cands[best].mb;
+    if (two_per_thread) *two_per_thread = cands[best].s2;
+    if (ms_out) *ms_out = best_ms;
+    return ESL_OK;
+}
+
 int esl_ctx_synchronize(esl_ctx* c) {
     if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
     ESL_CUDA(cudaStreamSynchronize(c->stream));

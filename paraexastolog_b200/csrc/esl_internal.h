@@ -118,6 +118,9 @@ struct esl_ctx {
     void* work = nullptr;             // solver workspace (grow-only), freed with the context
     void* sweep_work = nullptr;       // level-sweep workspace (grow-only), freed with the context
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // convergence polls of the level sweep
+    // level-sweep tiling of the last esl_net_autotune on this context (0 / -1: default),
+    // used for networks that have no tuning of their own
+    int tune_tile_mb = 0, tune_s2 = -1;
     // measurement hook: events around Schur-operator applications
     bool prof = false;
     struct ProfRec {
@@ -161,6 +164,9 @@ struct esl_net {
     void (*plan_free)(void*) = nullptr;
     // slot plan of the state-major level sweep, built on first use
     void* sweep = nullptr;
+    // level-sweep tiling picked by esl_net_autotune: L2 slice budget in MB (0: default)
+    // and two systems per thread on wide tiles (-1: default, on)
+    int tune_tile_mb = 0, tune_s2 = -1;
     void (*sweep_free)(void*) = nullptr;
     ~esl_net() {
         if (plan && plan_free) plan_free(plan);

@@ -1196,10 +1196,11 @@ double mixed_inner_rel() {
     return r;
 }
 
-int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0) {
+int tile_for(int Kp, int n, size_t elem, uint32_t rows = 0, size_t budget = 0) {
+    if (budget == 0) budget = tile_bytes();
     int kt = 128;
     while (kt > 32 && (Kp % kt != 0 || (size_t)2 * n * kt * elem > 36 * 1024 ||
-                       (size_t)rows * kt * elem > tile_bytes()))
+                       (size_t)rows * kt * elem > budget))
         kt >>= 1;
     return kt;
 }
@@ -1371,7 +1372,11 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         if (st_ != ESL_OK) return st_;
         double* X64 = Z + (size_t)(g.beg + g.ne) * Kp;  // the odd rows of the group, in place
         // tiles narrow enough that one tile's slice of a gathered vector stays in L2
-        const int gKT64 = tile_for(Kp, n, 8, std::max(g.ne, g.no)), gKT32 = tile_for(Kp, n, 4, std::max(g.ne, g.no));
+        // the network's autotuned slice budget, or the default
+        const int tmb = net->tune_tile_mb > 0 ? net->tune_tile_mb : ctx->tune_tile_mb;
+        const size_t budget = tmb > 0 ? (size_t)tmb << 20 : 0;
+        const int gKT64 = tile_for(Kp, n, 8, std::max(g.ne, g.no), budget),
+                  gKT32 = tile_for(Kp, n, 4, std::max(g.ne, g.no), budget);
         const size_t gsm64 = (size_t)2 * n * gKT64 * 8, gsm32 = (size_t)2 * n * gKT32 * 4;
         a.KT = gKT64;
         const dim3 ge = row_grid(g.ne, Kp, gKT64, ctx->sm_count), go = row_grid(g.no, Kp, gKT64, ctx->sm_count);
@@ -1495,7 +1500,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             const size_t smT = inner64 ? gsm64 : gsm32;
             const dim3 gei = row_grid(g.ne, Kp, a.KT, ctx->sm_count), goi = row_grid(g.no, Kp, a.KT, ctx->sm_count);
             // two systems per thread in the gather kernels when the tile is wide enough
-            const bool s2 = a.KT >= 64;
+            const bool s2 = a.KT >= 64 && (net->tune_s2 >= 0 ? net->tune_s2 != 0 : ctx->tune_s2 != 0);
             const dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2),
                        goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
             auto run_inner = [&](auto tag) -> int {

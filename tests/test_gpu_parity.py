@@ -317,3 +317,15 @@ def test_zanudo_golden_n23(esl, ctx, goldens):
     assert big.tolist() == c["nonzero_indices"]
     np.testing.assert_allclose(xi[big], c["nonzero_data"], atol=128 * FLT_EPS, rtol=0)
     assert abs(xi.sum() - 1.0) <= 1e-12
+
+
+def test_autotune_keeps_results(esl, ctx):
+    # the autotuner changes only the tiling: results stay within the solver tolerance
+    w = synth.config_precision(seed=3, n=14, n_rate_sets=96)
+    text, rates, x0 = w.networks[0].bnet, w.rates[0], w.x0[0]
+    net = esl.Net.build(ctx, esl.Model.parse(text), rates[0])
+    before = esl.solve_batch(ctx, net, rates, x0, method=esl.METHOD_DIRECT, tol=1e-12).x_inf.cpu().numpy()
+    pick = net.autotune(rates, x0, method=esl.METHOD_DIRECT, tol=1e-12)
+    assert pick["tile_mb"] in (16, 48, 128) and pick["ms"] > 0
+    after = esl.solve_batch(ctx, net, rates, x0, method=esl.METHOD_DIRECT, tol=1e-12).x_inf.cpu().numpy()
+    assert np.abs(after - before).sum(-1).max() <= 1e-10
