@@ -74,6 +74,7 @@ struct SweepPlan {
     int TS = 0;
     std::vector<SwGroup> groups;
     DevBuf<uint2> rows;                  // per slot: (state, out-mask)
+    DevBuf<uint4> desc;                  // per slot: (state, out-mask, first in-group entry, count)
     DevBuf<uint32_t> ig_ptr, ig_ent;     // predecessors inside the group: slot << 6 | rate index
     DevBuf<uint32_t> og_ptr, og_ent;     // predecessors in earlier groups
     DevBuf<uint32_t> tp_ptr, tp_ent;     // transient predecessors of terminal position p
@@ -88,6 +89,7 @@ struct SwArgs {
     int n, K, Kp, nrhs, KT;
     const double* rateT;     // [2n][Kp], rateT[j * Kp + k] = rate j of system k (0 past K)
     const uint2* rows;
+    const uint4* desc;       // per slot: (state, out-mask, first in-group entry, in-group count)
     const uint32_t* ig_ptr;
     const uint32_t* ig_ent;
     uint32_t beg, ne, no;
@@ -308,18 +310,15 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
     if (!__any_sync(0xffffffffu, any)) return;
     const uint32_t obase = a.beg + a.ne;
     for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne; r += gridDim.x * t.RB) {
-        const uint32_t slot = a.beg + r;
-        const uint2 row = a.rows[slot];
+        // (state, out-mask, first entry, count) in one load
+        const uint4 d = a.desc[a.beg + r];
         const size_t idx = (size_t)r * a.Kp + t.k;
         TC acc[S];
 #pragma unroll
         for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q * t.TR] : (TC)0;
-        if (X) {
-            const uint32_t p0 = a.ig_ptr[slot];
-            sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), X, obase, act, acc);
-        }
+        if (X) sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, X, obase, act, acc);
         TC qv[S];
-        sw_qs<S>(s_rate, row.x, row.y, t, qv);
+        sw_qs<S>(s_rate, d.x, d.y, t, qv);
 #pragma unroll
         for (int q = 0; q < S; q++)
             if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] / qv[q]);
@@ -357,16 +356,14 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
     }
     if (__any_sync(0xffffffffu, any)) {
         for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
-            const uint32_t slot = a.beg + a.ne + r;
-            const uint2 row = a.rows[slot];
+            const uint4 d = a.desc[a.beg + a.ne + r];  // (state, out-mask, first entry, count)
             const size_t idx = (size_t)r * a.Kp + t.k;
-            const uint32_t p0 = a.ig_ptr[slot];
             T flow[S];
 #pragma unroll
             for (int q = 0; q < S; q++) flow[q] = 0;
-            sw_gathers<S, T, T>(s_rate, t, a.Kp, a.ig_ent, p0, (int)(a.ig_ptr[slot + 1] - p0), W, a.beg, act, flow);
+            sw_gathers<S, T, T>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, W, a.beg, act, flow);
             T qv[S];
-            if (MODE != 0) sw_qs<S>(s_rate, row.x, row.y, t, qv);
+            if (MODE != 0) sw_qs<S>(s_rate, d.x, d.y, t, qv);
 #pragma unroll
             for (int q = 0; q < S; q++) {
                 if (!act[q]) continue;
@@ -1145,6 +1142,17 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
             cudaSuccess)
         rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
     up32(P->ig_ptr, ig_ptr);
+    {
+        std::vector<uint4> desc(M);
+        for (uint32_t sl = 0; sl < M; sl++)
+            desc[sl] = make_uint4(rows[sl].x, rows[sl].y, ig_ptr[sl], ig_ptr[sl + 1] - ig_ptr[sl]);
+        if (rc == ESL_OK) rc = P->desc.alloc(std::max<uint32_t>(M, 1));
+        if (rc == ESL_OK && M &&
+            cudaMemcpyAsync(P->desc.get(), desc.data(), (size_t)M * sizeof(uint4), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess)
+            rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
+        if (rc == ESL_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
+    }
     up32(P->ig_ent, ig);
     up32(P->og_ptr, og_ptr);
     up32(P->og_ent, og);
@@ -1308,6 +1316,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
     a.nrhs = nrhs;
     a.rateT = rateT;
     a.rows = P->rows.get();
+    a.desc = P->desc.get();
     a.ig_ptr = P->ig_ptr.get();
     a.ig_ent = P->ig_ent.get();
     int* h_cnt = reinterpret_cast<int*>(ctx->h_flag);  // pinned, at least 8 ints
