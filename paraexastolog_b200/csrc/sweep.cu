@@ -94,6 +94,10 @@ struct SwArgs {
     const uint32_t* ig_ent;
     uint32_t beg, ne, no;
     const int* flags;        // per-system flags or null
+    // FP64 out-rate sums of the group's rows, [row][Kp], or null (then recomputed from
+    // the out-masks): q of the odd rows and 1 / q of the even rows
+    const double* Qo;
+    const double* IQe;
 };
 
 // A tile is KT systems of one row handled by TR = KT / S threads, S systems per thread:
@@ -290,6 +294,24 @@ __global__ void __launch_bounds__(kSwT) k_sw_diag(SwArgs a, double* __restrict__
     }
 }
 
+// Out-rate sums of a grid group's rows, once per group: Qo = q of the odd rows, IQe =
+// 1 / q of the even rows, so that the operator kernels read one value per row and system
+// instead of summing the rates of the out-mask.
+__global__ void __launch_bounds__(kSwT) k_sw_qrows(SwArgs a, double* __restrict__ Qo, double* __restrict__ IQe) {
+    extern __shared__ double s_rate[];
+    const Tile t = tile_of(a.KT);
+    sw_rates(s_rate, a, t);
+    if (t.k >= a.K) return;
+    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne + a.no; r += gridDim.x * t.RB) {
+        const uint2 row = a.rows[a.beg + r];
+        const double q = sw_q(s_rate, row.x, row.y, t);
+        if (r < a.ne)
+            IQe[(size_t)r * a.Kp + t.k] = 1.0 / q;
+        else
+            Qo[(size_t)(r - a.ne) * a.Kp + t.k] = q;
+    }
+}
+
 // Even-row elimination: W_e = (C_e + sum over in-group odd predecessors o of
 // rate(o -> e) X_o) / q_e.  C (FP64, even rows of the group buffer) and X may be null.
 // S systems per thread.
@@ -317,11 +339,17 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
 #pragma unroll
         for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q * t.TR] : (TC)0;
         if (X) sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, X, obase, act, acc);
-        TC qv[S];
-        sw_qs<S>(s_rate, d.x, d.y, t, qv);
+        if (sizeof(TC) == 8 && a.IQe) {
 #pragma unroll
-        for (int q = 0; q < S; q++)
-            if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] / qv[q]);
+            for (int q = 0; q < S; q++)
+                if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] * (TC)__ldcs(a.IQe + idx + q * t.TR));
+        } else {
+            TC qv[S];
+            sw_qs<S>(s_rate, d.x, d.y, t, qv);
+#pragma unroll
+            for (int q = 0; q < S; q++)
+                if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] / qv[q]);
+        }
     }
 }
 
@@ -363,7 +391,14 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
             for (int q = 0; q < S; q++) flow[q] = 0;
             sw_gathers<S, T, T>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, W, a.beg, act, flow);
             T qv[S];
-            if (MODE != 0) sw_qs<S>(s_rate, d.x, d.y, t, qv);
+            if (MODE != 0) {
+                if (sizeof(T) == 8 && a.Qo) {
+#pragma unroll
+                    for (int q = 0; q < S; q++) qv[q] = act[q] ? (T)__ldcs(a.Qo + idx + q * t.TR) : (T)0;
+                } else {
+                    sw_qs<S>(s_rate, d.x, d.y, t, qv);
+                }
+            }
 #pragma unroll
             for (int q = 0; q < S; q++) {
                 if (!act[q]) continue;
@@ -977,7 +1012,7 @@ __global__ void k_sw_rate_table(int n, int K, int Kp, int nrhs, const double* __
 
 // ---- host side ------------------------------------------------------------------------------
 enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R, W_R0, W_PH, W_V, W_SH, W_TT,
-              W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_F0, W_COUNT = W_F0 + 8 };
+              W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_QO, W_IQE, W_F0, W_COUNT = W_F0 + 8 };
 
 bool debug_on();
 
@@ -1339,6 +1374,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_t0).count();
         };
         a.beg = g.beg;
+        a.Qo = a.IQe = nullptr;
         a.ne = g.ne;
         a.no = g.no;
         a.flags = nullptr;
@@ -1393,6 +1429,16 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         ESL_CUDA(cudaMemsetAsync(iscal, 0, (size_t)I_NISCAL * Kp * 4, s));
         ESL_COUNT_LAUNCH();
         k_sw_diag<<<go, kSwT, gsm64, s>>>(a, dS64, dS32);
+        if (g.kind == 2) {
+            // out-rate sums of the rows, read by the FP64 operator kernels of this group
+            double* Qo = (double*)ws.get(W_QO, vo * 8, &st_);
+            double* IQe = (double*)ws.get(W_IQE, ve * 8, &st_);
+            if (st_ != ESL_OK) return st_;
+            ESL_COUNT_LAUNCH();
+            k_sw_qrows<<<row_grid(g.ne + g.no, Kp, gKT64, ctx->sm_count), kSwT, gsm64, s>>>(a, Qo, IQe);
+            a.Qo = Qo;
+            a.IQe = IQe;
+        }
         // reduced rhs bS = b_odd + A_oe (b_even / q_e)
         ESL_COUNT_LAUNCH();
         k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, (const double*)nullptr, W64);
