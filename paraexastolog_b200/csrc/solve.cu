@@ -845,9 +845,8 @@ __global__ void k_zero_rows(Layout L, int parity, double* __restrict__ x) {
 }
 
 bool debug_enabled() {
-    static int on = -1;
-    if (on < 0) on = getenv("ESL_DEBUG") ? 1 : 0;
-    return on == 1;
+    static const bool on = getenv("ESL_DEBUG") != nullptr;
+    return on;
 }
 
 template <class T>

@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1017,6 +1018,9 @@ enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R,
 bool debug_on();
 
 int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
+    // one builder at a time, so that threads solving the same network share one plan
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
     if (net->sweep) {
         out = static_cast<SweepPlan*>(net->sweep);
         return ESL_OK;
@@ -1218,24 +1222,22 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
 // Krylov iteration hit L2.  The budget is a tuning parameter (ESL_SWEEP_TILE_MB,
 // default 48).
 size_t tile_bytes() {
-    static size_t b = 0;
-    if (b == 0) {
+    static const size_t b = [] {
         const char* e = getenv("ESL_SWEEP_TILE_MB");
         const long mb = e ? atol(e) : 0;
-        b = (size_t)(mb > 0 ? mb : 48) << 20;
-    }
+        return (size_t)(mb > 0 ? mb : 48) << 20;
+    }();
     return b;
 }
 
 // Relative residual target of an FP32 inner solve of the grid-wide groups, a tuning
 // parameter (ESL_MIXED_INNER_REL, default 1e-5).
 double mixed_inner_rel() {
-    static double r = 0.0;
-    if (r == 0.0) {
+    static const double r = [] {
         const char* e = getenv("ESL_MIXED_INNER_REL");
         const double v = e ? atof(e) : 0.0;
-        r = (v > 0.0 && v < 1.0) ? v : 1e-5;
-    }
+        return (v > 0.0 && v < 1.0) ? v : 1e-5;
+    }();
     return r;
 }
 
@@ -1277,9 +1279,8 @@ struct GraphPair {
 };
 
 bool debug_on() {
-    static int on = -1;
-    if (on < 0) on = getenv("ESL_DEBUG") ? 1 : 0;
-    return on == 1;
+    static const bool on = getenv("ESL_DEBUG") != nullptr;
+    return on;
 }
 
 }  // namespace
