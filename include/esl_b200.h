@@ -9,6 +9,9 @@
  *     else is host memory;
  *   - work is ordered on the stream given to esl_ctx_create; functions that
  *     return host results synchronise that stream;
+ *   - threads: one context per host thread at a time; a network may be solved from
+ *     several threads (on their own contexts) at once, its level-sweep plan is built
+ *     once under a lock and then only read;
  *   - state s is an n-bit integer, bit i is node i in bnet line order;
  *     rates are [up_0, down_0, ..., up_{n-1}, down_{n-1}] (FP64).
  */
