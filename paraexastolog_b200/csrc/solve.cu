@@ -35,6 +35,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "esl_internal.h"
 
@@ -1262,6 +1263,9 @@ __global__ void __launch_bounds__(256) k_dense_block(int n, const int32_t* __res
 }
 
 int get_plan(esl_ctx* ctx, const esl_net* net, BlockPlan*& out) {
+    // one builder at a time, so that threads solving the same network share one plan
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
     if (net->plan) {
         out = static_cast<BlockPlan*>(net->plan);
         return ESL_OK;
