@@ -18,6 +18,59 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+# entry point -> arguments of a call with NULL handles (C.c_double / c_float where the
+# signature has a floating-point argument, so that the call matches the ABI)
+_NULL_CALLS = {
+    "esl_ctx_synchronize": (None,),
+    "esl_model_parse": (None, None),
+    "esl_model_load": (None, None),
+    "esl_model_nodes": (None, None),
+    "esl_model_node_index": (None, None, None),
+    "esl_initial_state": (None, None, 0, None, None, 0, None, None, None),
+    "esl_table_nnz": (None, None, None, None),
+    "esl_table_build": (None, None, None, None, None, None),
+    "esl_flip_masks": (None, None, None, None, None),
+    "esl_net_build": (None, None, None, None),
+    "esl_net_info": (None, None, None, None, None),
+    "esl_net_export": (None, None, None, None, None, None),
+    "esl_net_autotune": (None, None, 1, None, 1, None, None, None, None, None),
+    "esl_net_compatible": (None, None, None),
+    "esl_solve": (None, None, None, None, None, None, None, None, None, None),
+    "esl_solve_batch": (None, None, 1, None, 1, None, None, None, None, None),
+    "esl_solve_many": (None, 0, None, 0, None),
+    "esl_mlp_create": (None, None, C.c_uint64(0), None),
+    "esl_mlp_info": (None, None, None, None),
+    "esl_mlp_targets": (None, None),
+    "esl_mlp_reach": (None, None),
+    "esl_mlp_get_params": (None, None),
+    "esl_mlp_set_params": (None, None, C.c_float(0.0), C.c_float(1.0)),
+    "esl_mlp_predict": (None, 1, None, None),
+    "esl_ctx_set_profiling": (None, 1),
+    "esl_ctx_profile": (None, None, None, None),
+    "esl_ctx_profile_records": (None, 0, None, None, None),
+    "esl_launch_count": (None,),
+}
+
+
+@pytest.mark.parametrize("name", sorted(_NULL_CALLS))
+def test_null_handles_are_rejected(name):
+    """Every entry point returns ESL_ERR_INVALID for NULL handles or outputs, before any
+    device work (this container has no GPU), and sets a message."""
+    f = getattr(esl.lib(), name)
+    f.restype = C.c_int
+    assert f(*_NULL_CALLS[name]) == -1
+    msg = esl.lib().esl_last_error
+    msg.restype = C.c_char_p
+    assert msg()
+
+
+@pytest.mark.parametrize("name", ["esl_ctx_destroy", "esl_model_free", "esl_net_free", "esl_mlp_free"])
+def test_free_of_null_is_a_no_op(name):
+    f = getattr(esl.lib(), name)
+    f.restype = C.c_int
+    assert f(None) == 0
+
+
 def _truth(off, pos, neg, i, states):
     f = np.zeros(len(states), bool)
     for c in range(off[i], off[i + 1]):
