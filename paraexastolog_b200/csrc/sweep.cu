@@ -48,6 +48,11 @@ constexpr int kSwLocalWarps = 16;    // most warps of a CTA-local solve
 constexpr int kSwPoll = 4;           // Krylov iterations launched between convergence polls
 constexpr double kSwAcceptRel = 1e-8;  // stagnating systems are accepted at this relative residual
 constexpr int kSwStall = 30;         // inner iterations without halving the residual before an inner solve stops
+// The same for the FP64 inner solves of grid-wide groups.  BiCGStab's residual there has
+// plateaus of up to ~90 iterations that end by themselves, and a restart discards the
+// Krylov space: on the largest group of the n=20 network, 30 cost three refinement rounds
+// and 376 iterations, 100 two rounds and 220 (512 rate sets, FP64 replica on the host).
+constexpr int kSwStall64 = 100;
 
 // per-system flags
 constexpr int SW_DONE = 1;   // group solve finished for this system
@@ -511,7 +516,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_xrp(SwArgs a, SwScalPtr sc, T* __re
 }
 
 // Scalar step after each iteration; one CTA; writes the number of running systems.
-__global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int* active) {
+__global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int stall_max, int* active) {
     __shared__ int s_cnt;
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
@@ -532,7 +537,7 @@ __global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int* active) {
             sc.i[I_STALL][k]++;
         }
         const bool stop = !(rr > sc.c[C_TARGET][k]) || it >= max_iters || r0v == 0.0 || omega == 0.0 ||
-                          rn == 0.0 || !isfinite(rr) || !isfinite(alpha) || sc.i[I_STALL][k] >= kSwStall;
+                          rn == 0.0 || !isfinite(rr) || !isfinite(alpha) || sc.i[I_STALL][k] >= stall_max;
         if (stop) {
             sc.i[I_FLAGS][k] = f | SW_IDONE;
         } else {
@@ -1618,7 +1623,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                     ESL_COUNT_LAUNCH();
                     k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                     ESL_COUNT_LAUNCH();
-                    k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, d_cnt + 1 + par);
+                    k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
+                                                 d_cnt + 1 + par);
                     }
                     ESL_CUDA(cudaGetLastError());
                     return ESL_OK;
