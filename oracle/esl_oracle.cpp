@@ -33,7 +33,9 @@
 // block.  Blocks larger than kDenseMax states are solved by FP64 BiCGStab with a
 // Jacobi preconditioner to a relative residual of 1e-14 -- not the reference's
 // algorithm (its dense/host LU has no feasible fill at that size); results at that
-// scale are flagged through eo_iterative_blocks() and eo_last_relres().
+// scale are flagged through eo_iterative_blocks() and eo_last_relres().  Terminal
+// SCCs of that size solve the rank-one deflated system (-K_C + u 1^T) pi = u,
+// which has the same solution as the row-replaced one (see terminal_kernel).
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -402,6 +404,7 @@ struct BlockOp {
     const std::vector<int32_t>* loc;  // global -> local, -1 outside the block
     bool transpose;
     std::vector<double> diag;
+    std::vector<double> u;  // optional rank-one term: y += u * (1^T x)
     void init() {
         diag.resize(mem->size());
         for (size_t a = 0; a < mem->size(); a++) {
@@ -427,6 +430,11 @@ struct BlockOp {
                 }
             }
             y[a] = acc;
+        }
+        if (!u.empty()) {
+            double sx = 0;
+            for (double xv : x) sx += xv;
+            for (size_t a = 0; a < u.size(); a++) y[a] += u[a] * sx;
         }
     }
 };
@@ -489,7 +497,7 @@ void block_solve(const Sym& g, const double* rates, const std::vector<int32_t>& 
                  std::vector<int32_t>& loc, bool transpose, std::vector<double>& rhs, int r) {
     int s = (int)mem.size();
     for (int a = 0; a < s; a++) loc[mem[a]] = a;
-    BlockOp op{&g, rates, &mem, &loc, transpose, {}};
+    BlockOp op{&g, rates, &mem, &loc, transpose, {}, {}};
     op.init();
     if (s <= kDenseMax) {
         std::vector<double> A((size_t)s * s, 0.0);
@@ -546,24 +554,22 @@ std::vector<double> terminal_kernel(const Sym& g, const double* rates, const std
         dense_solve(A, B, s, 1);
         pi = B;
     } else {
-        // fix pi[0] = 1: (-K) restricted to states 1..s-1 times pi_rest = K[rest, 0]
+        // Rank-one deflation: (-K_C + u 1^T) pi = u.  Because 1^T K_C = 0, any solution
+        // has 1^T pi = 1 and K_C pi = 0, the same kernel as the row-replaced system
+        // above.  The simple zero eigenvalue of -K_C moves to 1^T u and every other
+        // eigenvalue stays where it was (Brauer's theorem on the left eigenvector 1), so
+        // the conditioning follows the chain's spectral gap.  Fixing one state to 1
+        // instead makes the solution scale with 1 / pi(pinned state), which reached
+        // 1e78 on a 262,144-state attractor, with a residual relative to b that says
+        // nothing about the normalised kernel.  u = q / s puts 1^T u at the mean out-rate.
         g_iter_blocks++;
-        std::vector<int32_t> rest(mem.begin() + 1, mem.end());
-        loc[mem[0]] = -1;
-        for (int a = 0; a < s - 1; a++) loc[rest[a]] = a;
-        BlockOp op{&g, rates, &rest, &loc, true, {}};
+        BlockOp op{&g, rates, &mem, &loc, true, {}, {}};
         op.init();
-        std::vector<double> b(s - 1, 0.0), x(s - 1, 0.0);
-        uint32_t v0 = (uint32_t)mem[0];
-        for (int i = 0; i < g.n; i++)
-            if ((g.F[v0] >> i) & 1) {
-                int32_t a = loc[v0 ^ (1u << i)];
-                if (a >= 0) b[a] += edge_rate(rates, v0, i);
-            }
-        bicgstab(op, b, x, 1e-14, 50000);
-        pi[0] = 1.0;
-        for (int a = 0; a < s - 1; a++) pi[a + 1] = x[a];
-        for (int a = 0; a < s - 1; a++) loc[rest[a]] = -1;
+        op.u.resize(s);
+        for (int a = 0; a < s; a++) op.u[a] = op.diag[a] / s;
+        std::vector<double> x(s, 1.0 / s);
+        bicgstab(op, op.u, x, 1e-14, 50000);
+        pi = x;
     }
     for (int a = 0; a < s; a++) loc[mem[a]] = -1;
     double sum = 0;

@@ -1,0 +1,61 @@
+"""The oracle's terminal kernels of SCCs too large for its dense LU (more than 2,048
+states), which it solves by BiCGStab on the rank-one deflated system
+(-K_C + u 1^T) pi = u.  Checked against a closed form, and on the largest attractor
+of the many-network workload (n = 18: all 262,144 states in one terminal SCC) by the
+residual of the generator itself, which does not depend on how the system was posed."""
+import numpy as np
+
+import oracle as O
+from paraexastolog_b200 import synth
+
+
+def _generator_residual(F, rates, pi):
+    """|K pi|_1 / sum_v q_v pi_v for the generator K (K[dst, src] = rate, columns sum to 0)."""
+    n = int(np.log2(F.size))
+    s = np.arange(F.size, dtype=np.int64)
+    F = F.astype(np.int64)
+    Kpi = np.zeros(F.size)
+    outflow = np.zeros(F.size)
+    for b in range(n):
+        src = s[((F >> b) & 1) == 1]
+        up = ((src >> b) & 1) == 0
+        flow = np.where(up, rates[2 * b], rates[2 * b + 1]) * pi[src]
+        np.add.at(Kpi, src ^ (1 << b), flow)
+        outflow[src] += flow
+    Kpi -= outflow
+    return np.abs(Kpi).sum() / outflow.sum()
+
+
+def test_large_attractor_closed_form():
+    # every node negates itself: the whole 4,096-state cube is one terminal SCC and its
+    # kernel is the product of the per-node two-state chains
+    n = 12
+    m = O.Model(text="targets, factors\n" + "".join(f"v{i}, !v{i}\n" for i in range(n)))
+    rates = synth.log_uniform_rates(np.random.default_rng(5), n, 1)[0]
+    sym = m.analyse(rates)
+    assert sym.T == 1 and sym.N == 1 << n
+    pi = sym.terminal_kernels(rates)
+    assert O.iterative_blocks() == 1  # the iterative path, not the dense LU
+    s = np.arange(1 << n)
+    expect = np.ones(1 << n)
+    for i in range(n):
+        up, down = rates[2 * i], rates[2 * i + 1]
+        expect *= np.where((s >> i) & 1, up / (up + down), down / (up + down))
+    order = np.asarray(sym.order)
+    got = np.empty(1 << n)
+    got[order] = pi
+    np.testing.assert_allclose(got, expect, rtol=1e-11, atol=1e-15)
+
+
+def test_largest_attractor_of_the_many_network_workload():
+    w = synth.config_batch()
+    net, rates = w.networks[10], w.rates[10][0]
+    m = O.Model(text=net.bnet)
+    sym = m.analyse(rates)
+    assert sym.T == 1 and sym.N == 1 << 18 and sym.offsets[1] == sym.N
+    pi = sym.terminal_kernels(rates)
+    assert O.last_relres() <= 1e-13
+    assert abs(pi.sum() - 1.0) <= 1e-12 and pi.min() >= 0.0
+    full = np.empty(sym.N)
+    full[np.asarray(sym.order)] = pi
+    assert _generator_residual(np.asarray(m.flip_masks(rates)), rates, full) <= 1e-12
