@@ -4,7 +4,7 @@
 // network predicts, for a rate set k and a transient state v, the expected time z_k(v)
 // the chain spends in v before absorption (the occupation the level sweep solves for).
 // Its prediction is the starting iterate of the sweep's grid-wide Krylov groups
-// (esl_solve_opts.d_warm); the plain solve stays the judge of the result.
+// (esl_solve_opts.d_warm); the plain solve stays the arbiter of the result.
 //
 //   x(v, k) (77)  ->  h1 = relu(W1 x + b1) (128)  ->  h2 = relu(W2 h1 + b2) (128)
 //                 ->  y = w3 . h2 + b3,   z = exp(mu + sigma * y)

@@ -1,4 +1,4 @@
-"""The north-star configurations at their full sizes.
+"""The drop-in and precision workloads at their full sizes.
 
 n = 22 drop-in case (4,194,304 states, 535,520 SCCs, a 368,384-state transient SCC):
 the integer stages are bit-exact against the oracle (flip masks; order, offsets,
