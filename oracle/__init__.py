@@ -58,6 +58,7 @@ def lib():
     L.eo_solve.argtypes = [vp, f64p, f64p, f64p, f64p, C.c_int]
     L.eo_solve_many.argtypes = [vp, C.c_int, f64p, f64p, f64p, f64p, C.c_int]
     L.eo_initial_state.argtypes = [C.c_int, C.c_int, i32p, i32p, C.c_double, f64p]
+    L.eo_rates_normal.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, f64p, f64p, f64p]
     _lib = L
     return L
 
@@ -103,6 +104,20 @@ class Model:
             r[2 * self.names.index(name)] = v
         for name, v in (down or {}).items():
             r[2 * self.names.index(name) + 1] = v
+        return r
+
+    def rates_normal(self, mean, std, seed=0, up=None, down=None) -> np.ndarray:
+        """``transition_rates::generate_normal`` (``cuda/src/transition_rates.cpp:75-97``)."""
+        up_set = np.full(self.n, -1.0)
+        down_set = np.full(self.n, -1.0)
+        for name, v in (up or {}).items():
+            up_set[self.names.index(name)] = v
+        for name, v in (down or {}).items():
+            down_set[self.names.index(name)] = v
+        r = np.zeros(2 * self.n)
+        if lib().eo_rates_normal(self.n, float(mean), float(std), int(seed), _p(up_set, C.c_double),
+                                 _p(down_set, C.c_double), _p(r, C.c_double)) != 0:
+            raise OracleError(lib().eo_last_error().decode())
         return r
 
     def initial_state(self, fixed_names=(), fixed_values=(), p=1.0) -> np.ndarray:

@@ -26,6 +26,7 @@
 //   R, L, x_inf         cuda/src/solver.cu:102-309 (R = terminal kernels, L = [U | X]
 //                       absorption probabilities, x_inf = R (L x0))
 //   initial state       cuda/src/initial_state.cu:7-60
+//   normal rates        cuda/src/transition_rates.cpp:24-97 (eo_rates_normal)
 //
 // Numerics: terminal kernels solve K_C pi = 0 with one row replaced by the
 // normalisation row (dense LU with partial pivoting); the transient part is the
@@ -44,6 +45,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <random>
 #include <memory>
 #include <set>
 #include <sstream>
@@ -919,6 +921,36 @@ int eo_initial_state(int n, int n_fixed, const int32_t* nodes, const int32_t* va
     }
     for (uint64_t s = 0; s < N; s++)
         x0[s] = m[s] ? p / (double)match : (1.0 - p) / (double)(N - match);
+    return 0;
+}
+
+// Rates as in transition_rates::generate_normal (cuda/src/transition_rates.cpp:75-97)
+// through transition_rates::generate (:24-55): a default-constructed
+// std::default_random_engine (or one seeded with `seed` when it is not 0), a float
+// normal distribution, a negative draw redrawn up to 1000 times; nodes in order, up
+// before down, and a node's explicit rate (up_set / down_set >= 0: its value) takes no
+// draw.  Returns -1 when 1000 draws stay negative.
+int eo_rates_normal(int n, double mean, double stddev, uint64_t seed, const double* up_set, const double* down_set,
+                    double* out) {
+    std::default_random_engine gen;
+    if (seed) gen.seed((std::default_random_engine::result_type)seed);
+    std::normal_distribution<float> dist((float)mean, (float)stddev);
+    auto draw = [&](double& v) {
+        float x;
+        int count = 0;
+        do {
+            x = dist(gen);
+            count++;
+        } while (x < 0 && count < 1000);
+        v = x;
+        return x >= 0;
+    };
+    for (int i = 0; i < n; i++) {
+        if (up_set[i] >= 0) out[2 * i] = up_set[i];
+        else if (!draw(out[2 * i])) { g_error = "could not generate positive transition rates"; return -1; }
+        if (down_set[i] >= 0) out[2 * i + 1] = down_set[i];
+        else if (!draw(out[2 * i + 1])) { g_error = "could not generate positive transition rates"; return -1; }
+    }
     return 0;
 }
 

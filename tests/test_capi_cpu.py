@@ -133,3 +133,26 @@ def test_rates_host_api(goldens):
     b = m.rates_normal(1.0, 0.5)
     assert np.array_equal(a, b) and np.all(a >= 0)
     assert m.rates_normal(1.0, 0.5, up={"A": 7.0})[0] == 7.0
+
+
+@pytest.mark.parametrize("mean,std,seed", [(1.0, 0.5, 0), (0.2, 1.0, 0), (3.0, 2.0, 12345)])
+def test_rates_normal_matches_oracle(goldens, mean, std, seed):
+    # the same engine, distribution, redraw rule and draw order as the reference's
+    # generate_normal; (0.2, 1.0) redraws about 42% of the draws
+    for name in ("toy.bnet", "krasmodel15vars.bnet", "mammalian_cc.bnet"):
+        text = goldens["models"][name]
+        m, om = esl.Model.parse(text), O.Model(text=text)
+        assert m.rates_normal(mean, std, seed=seed).tolist() == om.rates_normal(mean, std, seed=seed).tolist()
+        # explicit rates take no draw: the following nodes get the draws the reference gives them
+        up, down = {om.names[0]: 7.0}, {om.names[-1]: 0.0, om.names[1]: 2.5}
+        got = m.rates_normal(mean, std, seed=seed, up=up, down=down)
+        assert got.tolist() == om.rates_normal(mean, std, seed=seed, up=up, down=down).tolist()
+        assert got[0] == 7.0 and got[-1] == 0.0 and got[3] == 2.5 and np.all(got >= 0)
+
+
+def test_rates_normal_gives_up_like_the_reference():
+    m, om = esl.Model.parse("A, A\nB, B\n"), O.Model(text="A, A\nB, B\n")
+    with pytest.raises(esl.EslError):
+        m.rates_normal(-50.0, 1.0)
+    with pytest.raises(O.OracleError):
+        om.rates_normal(-50.0, 1.0)
