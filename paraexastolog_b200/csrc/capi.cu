@@ -43,7 +43,9 @@ int check_rates(const Model& m, const double* rates) {
 
 int rate_map(const Model& m, int count, const char* const* names, const double* vals, std::vector<int>& idx) {
     idx.assign(m.n(), -1);
+    if (count < 0 || (count > 0 && (!names || !vals))) return fail(ESL_ERR_INVALID, "bad explicit rate list");
     for (int k = 0; k < count; k++) {
+        if (!names[k]) return fail(ESL_ERR_INVALID, "explicit rate without a node name");
         int found = -1;
         for (int i = 0; i < m.n(); i++)
             if (m.names[i] == names[k]) {
@@ -354,6 +356,7 @@ int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char*
     const uint64_t N = 1ull << n;
     uint32_t mask = 0, val = 0;
     for (int k = 0; k < n_fixed; k++) {
+        if (!fixed_names[k]) return fail(ESL_ERR_INVALID, "fixed node without a name");
         int idx = -1;
         for (int i = 0; i < n; i++)
             if (m->m.names[i] == fixed_names[k]) {

@@ -156,3 +156,22 @@ def test_rates_normal_gives_up_like_the_reference():
         m.rates_normal(-50.0, 1.0)
     with pytest.raises(O.OracleError):
         om.rates_normal(-50.0, 1.0)
+
+
+def test_explicit_rate_lists_are_checked():
+    """A count with a NULL name or value array, or a NULL name inside it, is an error
+    rather than a dereference."""
+    m = esl.Model.parse("A, A\nB, !A\n")
+    out = np.zeros(4)
+    f = esl.lib().esl_rates_uniform
+    name = C.c_char_p(b"A")
+    names = (C.c_char_p * 1)(name)
+    vals = np.array([2.0])
+    assert f(m._h, 1, None, vals.ctypes.data, 0, None, None, out.ctypes.data) == -1
+    assert f(m._h, 1, names, None, 0, None, None, out.ctypes.data) == -1
+    assert f(m._h, 0, None, None, -1, None, None, out.ctypes.data) == -1
+    assert f(m._h, 1, (C.c_char_p * 1)(None), vals.ctypes.data, 0, None, None, out.ctypes.data) == -1
+    assert f(m._h, 1, names, vals.ctypes.data, 0, None, None, out.ctypes.data) == 0
+    assert out.tolist() == [2.0, 1.0, 1.0, 1.0]
+    g = esl.lib().esl_rates_normal
+    assert g(m._h, 1.0, 0.5, 0, 0, None, None, 1, None, vals.ctypes.data, out.ctypes.data) == -1
