@@ -423,6 +423,7 @@ int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32
 int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net** out) {
     if (!ctx || !m || !out) return fail(ESL_ERR_INVALID, "NULL argument");
     *out = nullptr;
+    ESL_TRY(check_rates(m->m, rates));
     auto* net = new esl_net();
     net->n = m->m.n();
     net->N = 1ll << net->n;
