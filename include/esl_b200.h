@@ -175,7 +175,9 @@ int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rat
  *      the contexts of the pool (each with its own stream and workspace; create them on
  *      one device or several) run the jobs concurrently from host threads, largest
  *      first, so that small networks overlap on the GPU.  Returns the first failing
- *      job's status; every job's status and report are written back. */
+ *      job's status; every job's status and report are written back.  A context whose
+ *      device cannot be selected takes no job and makes the call return ESL_ERR_CUDA;
+ *      the other contexts still run the jobs. */
 typedef struct esl_job {
     const esl_net* net;
     int B;                   /* rate sets (d_rates B x 2n, same zero pattern as net) */

@@ -55,7 +55,16 @@ extern "C" int esl_solve_many(esl_ctx* const* ctxs, int n_ctx, esl_job* jobs, in
     std::string first_msg;
     auto worker = [&](int c) {
         esl_ctx* ctx = ctxs[c];
-        if (cudaSetDevice(ctx->device) != cudaSuccess) return;
+        const cudaError_t e = cudaSetDevice(ctx->device);
+        if (e != cudaSuccess) {
+            // this worker takes no job; the others drain the queue
+            std::lock_guard<std::mutex> lk(mu);
+            if (first_status == ESL_OK) {
+                first_status = ESL_ERR_CUDA;
+                first_msg = std::string("context ") + std::to_string(c) + ": cudaSetDevice: " + cudaGetErrorString(e);
+            }
+            return;
+        }
         for (;;) {
             const int i = next.fetch_add(1);
             if (i >= n_jobs) break;
@@ -77,6 +86,8 @@ extern "C" int esl_solve_many(esl_ctx* const* ctxs, int n_ctx, esl_job* jobs, in
     const int nt = std::min(n_ctx, n_jobs);
     for (int c = 0; c < nt; c++) th.emplace_back(worker, c);
     for (auto& t : th) t.join();
+    // jobs that no worker took (every worker failed to select its device)
+    for (int i = std::min(next.load(), n_jobs); i < n_jobs; i++) jobs[order[i]].status = first_status;
     if (first_status != ESL_OK) return fail(first_status, first_msg);
     return ESL_OK;
 }
