@@ -78,31 +78,32 @@ class RuleParser {
         return r;
     }
     // Parse tree; the DNF is derived from it with negations pushed to the leaves.
+    // '|' and '&' chains are n-ary nodes built by loops, so the depth of the parser's
+    // recursion, of the tree and of to_dnf follows the parenthesis nesting, which is
+    // limited, and not the length of a chain.  Folding an n-ary node left to right
+    // gives the terms in the same order as the grammar's right-recursive reading
+    // (concatenation for '|', the lexicographic cross product for '&').
     struct Tree {
         int kind;  // 0 var, 1 not, 2 and, 3 or
         int id;
-        std::unique_ptr<Tree> l, r;
+        std::vector<std::unique_ptr<Tree>> kids;
     };
-    std::unique_ptr<Tree> texpr() {
-        auto l = tterm();
-        if (!peek('|')) return l;
-        ++i_;
+    static constexpr int kMaxNesting = 512;
+    int depth_ = 0;
+    std::unique_ptr<Tree> chain(int kind, char op, std::unique_ptr<Tree> (RuleParser::*next)()) {
+        auto first = (this->*next)();
+        if (!peek(op)) return first;
         auto t = std::make_unique<Tree>();
-        t->kind = 3;
-        t->l = std::move(l);
-        t->r = texpr();
+        t->kind = kind;
+        t->kids.push_back(std::move(first));
+        while (peek(op)) {
+            ++i_;
+            t->kids.push_back((this->*next)());
+        }
         return t;
     }
-    std::unique_ptr<Tree> tterm() {
-        auto l = tfactor();
-        if (!peek('&')) return l;
-        ++i_;
-        auto t = std::make_unique<Tree>();
-        t->kind = 2;
-        t->l = std::move(l);
-        t->r = tterm();
-        return t;
-    }
+    std::unique_ptr<Tree> texpr() { return chain(3, '|', &RuleParser::tterm); }
+    std::unique_ptr<Tree> tterm() { return chain(2, '&', &RuleParser::tfactor); }
     std::unique_ptr<Tree> tfactor() {
         int nots = 0;
         while (peek('!')) {
@@ -113,15 +114,17 @@ class RuleParser {
         if (nots % 2 == 0) return a;
         auto t = std::make_unique<Tree>();
         t->kind = 1;
-        t->r = std::move(a);
+        t->kids.push_back(std::move(a));
         return t;
     }
     std::unique_ptr<Tree> tatom() {
         if (peek('(')) {
             ++i_;
+            if (++depth_ > kMaxNesting) throw std::runtime_error("expression nested too deeply");
             auto e = texpr();
             if (!peek(')')) throw std::runtime_error("runaway parenthesis");
             ++i_;
+            --depth_;
             return e;
         }
         ws();
@@ -151,12 +154,15 @@ class RuleParser {
                 return {l};
             }
             case 1:
-                return to_dnf(t->r.get(), !neg);
+                return to_dnf(t->kids[0].get(), !neg);
             default: {
                 bool is_or = (t->kind == 3) != neg;
-                auto a = to_dnf(t->l.get(), neg);
-                auto b = to_dnf(t->r.get(), neg);
-                return is_or ? disj(std::move(a), b) : conj(a, b);
+                auto acc = to_dnf(t->kids[0].get(), neg);
+                for (size_t k = 1; k < t->kids.size(); k++) {
+                    auto b = to_dnf(t->kids[k].get(), neg);
+                    acc = is_or ? disj(std::move(acc), b) : conj(acc, b);
+                }
+                return acc;
             }
         }
     }

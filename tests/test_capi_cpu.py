@@ -175,3 +175,19 @@ def test_explicit_rate_lists_are_checked():
     assert out.tolist() == [2.0, 1.0, 1.0, 1.0]
     g = esl.lib().esl_rates_normal
     assert g(m._h, 1.0, 0.5, 0, 0, None, None, 1, None, vals.ctypes.data, out.ctypes.data) == -1
+
+
+def test_long_chains_and_deep_nesting():
+    """Chains of any length parse (they used to recurse once per operator and overflow
+    the stack); parenthesis nesting beyond 512 levels is a parse error, not a crash."""
+    k = 200_000
+    for text in (" | ".join(["A"] * k), " & ".join(["A"] * k), "(" * 512 + "!!A" + ")" * 512):
+        m = esl.Model.parse("targets, factors\nA, " + text + "\nB, A | B\n")
+        off, pos, neg = m.clauses()
+        assert off.tolist() == [0, 1, 3] and pos[0] == 1 and neg[0] == 0
+    for depth in (513, k):
+        with pytest.raises(esl.EslError, match="nested too deeply"):
+            esl.Model.parse("targets, factors\nA, " + "(" * depth + "A" + ")" * depth + "\n")
+    # the same rule written flat and as a long mixed chain gives the oracle's clauses
+    _same_clauses("targets, factors\nA, " + " | ".join(f"(A & !B & C{i % 3})" for i in range(3000)) +
+                  "\nB, B\nC0, A\nC1, B\nC2, C0\n")
