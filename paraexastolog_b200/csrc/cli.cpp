@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -173,7 +174,9 @@ int parse(int argc, char** argv, Args& a) {
             else if (v == "fp64") a.method = ESL_METHOD_FP64;
             else return 1;
         } else if (o == "--seed") {
-            if (!value(v) || !number(v, x) || x < 0) return 1;
+            // a whole number that a uint64_t holds (NaN and 2^64 or more are rejected)
+            if (!value(v) || !number(v, x) || !(x >= 0.0 && x < 18446744073709551616.0) || x != std::floor(x))
+                return 1;
             a.seed = (uint64_t)x;
         } else {
             return 1;

@@ -44,3 +44,9 @@ def test_bad_transition_rates(cli, bad):
 def test_bad_fixed_list(cli, bad):
     rc, _, err = _run(cli, "-f", "x.bnet", "--initial-fixed-list", bad)
     assert rc == 1 and "usage" in err
+
+
+@pytest.mark.parametrize("bad", ["-1", "nan", "1e30", "2.5", "x"])
+def test_bad_seed(cli, bad):
+    rc, _, err = _run(cli, "-f", "x.bnet", "--seed", bad)
+    assert rc == 1 and "usage" in err
