@@ -240,6 +240,8 @@ bool read_symb(const std::string& path, Symb& s) {
     size_t sz[16];
     f.read(reinterpret_cast<char*>(sz), sizeof sz);
     size_t idx = 0, real = 0;
+    for (size_t v : sz)
+        if (v > (size_t)len) return false;  // keeps the sums below from wrapping
     for (int i : {0, 1, 2, 3, 4, 5, 7, 8, 10, 11, 13, 14}) idx += sz[i];
     for (int i : {6, 9, 12, 15}) real += sz[i];
     if ((size_t)len != idx * sizeof(int32_t) + real * sizeof(float) + sizeof sz) return false;
@@ -255,6 +257,19 @@ bool read_symb(const std::string& path, Symb& s) {
     get(s.nonterm_off, sz[5]);
     get(s.rates, sz[6]);
     return (bool)f;
+}
+
+// A stored table is used only if it is a well-formed CSC over the N states: the
+// kernels that read it index rows[] through indptr[] without bounds checks, so a stale
+// or damaged file must be turned away here.
+bool valid_csc(const Symb& s, size_t N) {
+    if (s.indptr.size() != N + 1 || s.indptr[0] != 0) return false;
+    for (size_t v = 0; v < N; v++)
+        if (s.indptr[v + 1] < s.indptr[v]) return false;
+    if ((size_t)s.indptr[N] != s.rows.size()) return false;
+    for (int32_t r : s.rows)
+        if (r < 0 || (size_t)r >= N) return false;
+    return true;
 }
 
 std::string symb_path(const std::string& bnet) {
@@ -321,7 +336,7 @@ int run(const Args& a) {
     const std::string sp = symb_path(a.bnet);
     Symb stored;
     bool reuse = false, same_rates = false;
-    if (a.symbolic && read_symb(sp, stored) && stored.rates.size() == rates.size() && stored.indptr.size() == N + 1) {
+    if (a.symbolic && read_symb(sp, stored) && stored.rates.size() == rates.size() && valid_csc(stored, N)) {
         bool zeros_in_stored = false;
         reuse = true;
         same_rates = true;

@@ -132,3 +132,27 @@ def test_cli_symbolic_file(esl, cli, goldens, tmp_path):
     assert _run(cli, path, "-s", *other) == _run(cli, path, *other)
     _, arrays = _read_symb(symb)
     assert arrays[6][0] == np.float32(2.5)
+
+
+def test_cli_turns_away_a_damaged_symbolic_file(esl, cli, goldens, tmp_path):
+    # a stored table whose column pointers do not end at its edge count is not
+    # uploaded (the kernels that read it index rows through them unchecked): the run
+    # builds the table itself, prints what a run without -s prints and rewrites the file
+    text = goldens["models"]["krasmodel15vars.bnet"]
+    path = tmp_path / "kras.bnet"
+    path.write_text(text)
+    symb = tmp_path / "kras.symb"
+    plain = _run(cli, path)
+    assert _run(cli, path, "-s") == plain
+    good = symb.read_bytes()
+    sizes, arrays = _read_symb(symb)
+    indptr_last = 128 + 4 * (sizes[0] + sizes[1] + sizes[2] - 1)
+    assert struct.unpack_from("<i", good, indptr_last)[0] == arrays[2][-1] == sizes[0]
+    bad = bytearray(good)
+    struct.pack_into("<i", bad, indptr_last, int(sizes[0]) + 1000)
+    symb.write_bytes(bytes(bad))
+    assert _run(cli, path, "-s") == plain
+    sizes2, arrays2 = _read_symb(symb)
+    assert sizes2 == sizes
+    for k in range(7):  # table, order, SCC offsets and rates as first written
+        assert np.array_equal(arrays2[k], arrays[k]), k
