@@ -136,7 +136,11 @@ int esl_table_build_static(const esl_model* m, const double* rates, void* cuda_s
  *      (cuda/src/transition_graph.cu:39-202, kernels/transition_graph.cu:3-52).
  *      Builds table masks, SCCs, terminal SCCs, levels and the reordering on the device. */
 int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net** out);
-/* same from a CSC table (any single-bit-flip graph, e.g. one produced by esl_table_build) */
+/* same from a CSC table (any single-bit-flip graph, e.g. one produced by esl_table_build).
+ * The table is read on the device as given: d_indptr (2^n + 1 entries) must start at 0
+ * and never decrease, and d_rows must hold d_indptr[2^n] entries.  Edges that do not
+ * flip exactly one bit of their source are reported (ESL_ERR_INVALID); pointers are not
+ * checked, so validate a table from an untrusted source before the call. */
 int esl_net_from_csc(esl_ctx* ctx, int n_nodes, const int32_t* d_indptr, const int32_t* d_rows,
                      esl_net** out);
 int esl_net_free(esl_net* net);
