@@ -220,7 +220,9 @@ int esl_mlp_targets(const esl_mlp* mlp, uint32_t* d_states);  /* n_targets state
 int esl_mlp_reach(const esl_mlp* mlp, uint32_t* d_reach);     /* N words: bit t = reaches terminal t */
 int esl_mlp_get_params(const esl_mlp* mlp, float* params);    /* host, ESL_MLP_PARAMS floats */
 int esl_mlp_set_params(esl_mlp* mlp, const float* params, float mu, float sigma);
-/* feature rows (S x 80 floats, device) of samples (rate set d_k[s] of d_rates, state d_state[s]) */
+/* feature rows (S x 80 floats, device) of samples (rate set d_k[s] of d_rates, state d_state[s]).
+ * Here and in esl_mlp_loss_grad / esl_mlp_forward the sample indices are read on the
+ * device unchecked: 0 <= d_k[s] < the rate sets in d_rates, 0 <= d_state[s] < 2^n. */
 int esl_mlp_features(esl_mlp* mlp, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
                      float* d_x);
 /* mean squared error against standardized targets and, if grad != NULL, its gradient
