@@ -59,3 +59,31 @@ def test_largest_attractor_of_the_many_network_workload():
     full = np.empty(sym.N)
     full[np.asarray(sym.order)] = pi
     assert _generator_residual(np.asarray(m.flip_masks(rates)), rates, full) <= 1e-12
+
+
+def test_large_transient_block_closed_form():
+    # v0 latches on from the all-ones corner of the free nodes, v1 from the all-zeros
+    # corner; the other nodes flip freely.  Terminal SCCs: (v0, v1) = (1, 0), (0, 1) and
+    # (1, 1), each uniform over the 4,096 states of the free nodes; the 4,096-state block
+    # (0, 0) is transient.  With equal rates, swapping v0 and v1 and complementing the
+    # free nodes maps the chain to itself, so the block's mass splits evenly: from a
+    # uniform x0, (1, 0) and (0, 1) end with 3/8 each and (1, 1) keeps its 1/4.
+    n = 14
+    free = range(2, n)
+    text = ("targets, factors\n"
+            f"v0, v0 | (!v1 & {' & '.join(f'v{i}' for i in free)})\n"
+            f"v1, v1 | (!v0 & {' & '.join(f'!v{i}' for i in free)})\n" +
+            "".join(f"v{i}, !v{i}\n" for i in free))
+    m = O.Model(text=text)
+    rates = m.rates()
+    sym = m.analyse(rates)
+    assert sym.T == 3 and sym.n_sccs == 4
+    x, marg = sym.solve(m.initial_state(), rates)
+    assert O.iterative_blocks() >= 1
+    s = np.arange(1 << n)
+    b0, b1 = s & 1, (s >> 1) & 1
+    expect = np.where(b0 & ~b1 & 1, 0.375, 0.0) + np.where(~b0 & b1 & 1, 0.375, 0.0) + np.where(b0 & b1, 0.25, 0.0)
+    expect /= 1 << (n - 2)
+    assert np.abs(x - expect).sum() <= 1e-10
+    np.testing.assert_allclose(marg[:2], [0.625, 0.625], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(marg[2:], 0.5, rtol=0, atol=1e-11)
