@@ -191,3 +191,33 @@ def test_long_chains_and_deep_nesting():
     # the same rule written flat and as a long mixed chain gives the oracle's clauses
     _same_clauses("targets, factors\nA, " + " | ".join(f"(A & !B & C{i % 3})" for i in range(3000)) +
                   "\nB, B\nC0, A\nC1, B\nC2, C0\n")
+
+
+def _random_rule(rng, depth=0):
+    atoms = ["A", "B", "C", "D"] * 3 + ["X", "Y", "1", "0", "true", "n_1"]
+    if depth > 3 or rng.random() < 0.3:
+        return "!" * int(rng.integers(0, 3)) + atoms[rng.integers(len(atoms))]
+    op = " & " if rng.random() < 0.5 else " | "
+    body = op.join(_random_rule(rng, depth + 1) for _ in range(int(rng.integers(2, 4))))
+    return "!" * int(rng.integers(0, 2)) + "(" + body + ")" if rng.random() < 0.7 else body
+
+
+def test_parser_fuzz_against_oracle():
+    """Random rules (nesting, negation chains, identifiers that are not nodes, constants,
+    contradictions, uneven spacing): the library and the oracle either both reject a
+    model or give every node the same truth function."""
+    rng = np.random.default_rng(0)
+    agree = rejected = 0
+    for _ in range(300):
+        text = "targets, factors\n" + "".join(
+            f"{n},{' ' * int(rng.integers(0, 3))}{_random_rule(rng)}\n" for n in "ABCD")
+        try:
+            esl.Model.parse(text)
+        except esl.EslError:
+            with pytest.raises(O.OracleError):
+                O.Model(text=text)
+            rejected += 1
+            continue
+        _same_clauses(text)
+        agree += 1
+    assert agree >= 250 and rejected >= 1
