@@ -163,6 +163,39 @@ def parse_test_cu(ref: str):
     return cases
 
 
+def uniformized_limit(text: str) -> np.ndarray:
+    """lim_{t->inf} exp(K t) x0 for the uniform x0 and uniform rates, by repeated
+    squaring of the uniformized chain P = I + K / q (q above every exit rate, so P is
+    aperiodic), columns renormalised after each squaring.  Dense, for small n only.
+    It uses the transition table alone (the oracle's flip masks, which the reference's
+    table goldens pin) and none of the SCC or solver logic, so it can judge a result of
+    the Python path independently of the oracle's solve."""
+    sys.path.insert(0, REPO)
+    import oracle as O
+    m = O.Model(text=text)
+    r = m.rates()
+    N = 1 << m.n
+    F = np.asarray(m.flip_masks(r)).astype(np.int64)
+    K = np.zeros((N, N))
+    s = np.arange(N)
+    for b in range(m.n):
+        src = s[((F >> b) & 1) == 1]
+        rate = np.where(((src >> b) & 1) == 0, r[2 * b], r[2 * b + 1])
+        K[src ^ (1 << b), src] += rate
+        K[src, src] -= rate
+    P = np.eye(N) + K / (1.5 * max(-K.diagonal().min(), 1e-300))
+    x0 = np.full(N, 1.0 / N)
+    prev = None
+    for _ in range(64):
+        P = P @ P
+        P /= P.sum(0, keepdims=True)
+        x = P @ x0
+        if prev is not None and np.abs(x - prev).sum() <= 1e-15:
+            break
+        prev = x
+    return x
+
+
 def python_reference(ref: str, models: dict, max_nodes: int = 12):
     """x_inf of the reference's Python path for uniform rates and uniform x0."""
     sys.modules.setdefault("pyeda", types.ModuleType("pyeda"))
@@ -194,10 +227,19 @@ def python_reference(ref: str, models: dict, max_nodes: int = 12):
             graph = ex.TransitionGraph(table, init)
             graph.sort()
             sol = ex.Solution(graph, init, len(model.model.keys()))
-            x = np.asarray(sol.compute_final_states(), dtype=float)
+            try:
+                x = np.asarray(sol.compute_final_states(), dtype=float)
+            except Exception as e:  # the Python path's own failure: recorded, not a golden
+                out[key] = {"valid": False, "error": f"{type(e).__name__}: {e}",
+                            "source": "python/exastolog.py (shimmed)"}
+                continue
             nz = np.nonzero(x)[0]
+            # valid only where it matches the uniformized limit (a sum of 1 is not
+            # enough: the path can misplace mass and still sum to 1)
+            l1 = float(np.abs(x - uniformized_limit(text)).sum())
             out[key] = {"nonzero_indices": nz.tolist(), "nonzero_data": x[nz].tolist(),
-                        "valid": bool(abs(x.sum() - 1.0) < 1e-9), "source": "python/exastolog.py (shimmed)"}
+                        "valid": bool(abs(x.sum() - 1.0) < 1e-9 and l1 <= 1e-9), "l1_vs_uniformized_limit": l1,
+                        "source": "python/exastolog.py (shimmed)"}
         finally:
             os.unlink(path)
     return out
@@ -218,13 +260,37 @@ def main():
     sys.path.insert(0, REPO)
     from paraexastolog_b200 import synth
     gen = {"synth.n10_k2_uniform": synth.config_small().networks[0].bnet}
+    # seeded random uniform-rate networks whose terminal SCCs are small enough for the
+    # Python path's O(s^4) cofactor kernels (at most 64 states)
+    import oracle as O
+    rng = np.random.default_rng(20)
+    while len(gen) < 25:
+        n = int(rng.integers(6, 11))
+        text = synth.random_table_network(rng, n, [1, 2, 3], 0.5).bnet
+        m = O.Model(text=text)
+        sym = m.analyse(m.rates())
+        if np.diff(sym.offsets[: sym.T + 1]).max() <= 64:
+            gen[f"synth.random_{len(gen)}_n{n}"] = text
     pyref_models = dict(small)
     pyref_models.update(gen)
     pyref_models["toy.bnet"] = models["toy.bnet"]
     pyref_models["krasmodel15vars.bnet"] = models["krasmodel15vars.bnet"]
     pyref = python_reference(ref, pyref_models)
 
-    out = {"models": models, "generated_models": gen, "cases": cases, "python_ref": pyref}
+    # the uniformized limit of every model the Python path ran on: an exact answer for
+    # uniform rates and x0 that does not depend on any solver, including where that
+    # path is wrong
+    limits = {}
+    for key, text in pyref_models.items():
+        if key not in pyref:
+            continue
+        x = uniformized_limit(text)
+        nz = np.nonzero(x > 1e-15)[0]  # entries below count for nothing at the tests' 1e-10
+        limits[key] = {"nonzero_indices": nz.tolist(), "nonzero_data": x[nz].tolist(),
+                       "source": "uniformized chain, repeated squaring (make_golden.uniformized_limit)"}
+
+    out = {"models": models, "generated_models": gen, "cases": cases, "python_ref": pyref,
+           "uniformized_limits": limits}
     with open(os.path.join(HERE, "reference_goldens.json"), "w") as f:
         json.dump(out, f, indent=0)
     print("cases:", len(cases), "python_ref:", {k: v["valid"] for k, v in pyref.items()})

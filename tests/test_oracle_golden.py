@@ -113,6 +113,24 @@ def test_python_reference_fixtures(goldens):
     assert checked >= 5
 
 
+def test_uniformized_limits(goldens):
+    """The oracle against the limit of the uniformized chain (uniform rates and x0),
+    computed by repeated squaring with no SCC or solver logic, for every model the
+    Python path was run on -- including the ones where that path is wrong."""
+    checked = wrong_python = 0
+    for key, lim in goldens["uniformized_limits"].items():
+        text = goldens["models"].get(key) or goldens["generated_models"].get(key)
+        m = O.Model(text=text)
+        s = m.analyse(m.rates())
+        xi, _ = s.solve(m.initial_state())
+        exact = np.zeros(1 << m.n)
+        exact[lim["nonzero_indices"]] = lim["nonzero_data"]
+        assert np.abs(xi - exact).sum() <= 1e-10, key
+        checked += 1
+        wrong_python += not goldens["python_ref"][key]["valid"]
+    assert checked >= 30 and wrong_python >= 10
+
+
 def test_bnet_quirks():
     # header skipped only when it starts with "targets"; unterminated last line dropped
     m = O.Model(text="targets, factors\nA, A\nB, !A")
