@@ -1,8 +1,12 @@
-"""The oracle's terminal kernels of SCCs too large for its dense LU (more than 2,048
-states), which it solves by BiCGStab on the rank-one deflated system
-(-K_C + u 1^T) pi = u.  Checked against a closed form, and on the largest attractor
-of the many-network workload (n = 18: all 262,144 states in one terminal SCC) by the
-residual of the generator itself, which does not depend on how the system was posed."""
+"""The oracle against exact answers that need no solver.
+
+- Terminal kernels of SCCs too large for its dense LU (more than 2,048 states), which
+  it solves by BiCGStab on the rank-one deflated system (-K_C + u 1^T) pi = u: a closed
+  form, and the generator residual on the largest attractor of the many-network
+  workload (n = 18: all 262,144 states in one terminal SCC).
+- The iterative transient path: a closed form from a symmetry of the chain.
+- Per-node rates (some zero) and non-uniform x0 on small networks: the limit of the
+  uniformized chain by repeated squaring."""
 import numpy as np
 
 import oracle as O
@@ -87,3 +91,39 @@ def test_large_transient_block_closed_form():
     assert np.abs(x - expect).sum() <= 1e-10
     np.testing.assert_allclose(marg[:2], [0.625, 0.625], rtol=0, atol=1e-11)
     np.testing.assert_allclose(marg[2:], 0.5, rtol=0, atol=1e-11)
+
+
+def _limit(F, rates, x0):
+    """lim exp(K t) x0 by repeated squaring of the uniformized chain (columns renormalised);
+    uses the transition table only."""
+    n = int(np.log2(F.size))
+    N = F.size
+    s = np.arange(N, dtype=np.int64)
+    F = F.astype(np.int64)
+    K = np.zeros((N, N))
+    for b in range(n):
+        src = s[((F >> b) & 1) == 1]
+        rate = np.where(((src >> b) & 1) == 0, rates[2 * b], rates[2 * b + 1])
+        K[src ^ (1 << b), src] += rate
+        K[src, src] -= rate
+    P = np.eye(N) + K / (1.5 * max(-K.diagonal().min(), 1e-300))
+    for _ in range(80):
+        P = P @ P
+        P /= P.sum(0, keepdims=True)
+    return P @ x0
+
+
+def test_oracle_matches_the_uniformized_limit_with_rates():
+    # per-node log-uniform rates, some of them zero, and Dirichlet x0 over a node subset:
+    # the cases the reference's Python path cannot solve (it ignores rates)
+    rng = np.random.default_rng(11)
+    for _ in range(12):
+        n = int(rng.integers(5, 9))
+        net = synth.random_table_network(rng, n, [1, 2, 3], 0.5)
+        rates = synth.log_uniform_rates(rng, n, 1)[0]
+        rates[rng.choice(2 * n, 2, replace=False)] = 0.0
+        x0 = synth.dirichlet_subspace_x0(rng, n, rng.choice(n, 3, replace=False))
+        m = O.Model(text=net.bnet)
+        x, _ = m.analyse(rates).solve(x0, rates)
+        exact = _limit(np.asarray(m.flip_masks(rates)), rates, x0)
+        assert np.abs(x - exact).sum() <= 1e-10
