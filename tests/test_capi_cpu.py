@@ -221,3 +221,24 @@ def test_parser_fuzz_against_oracle():
         _same_clauses(text)
         agree += 1
     assert agree >= 250 and rejected >= 1
+
+
+def test_node_count_limits():
+    """30 nodes (ESL_MAX_NODES) parse; 31 are ESL_ERR_TOO_LARGE; an empty model is a
+    parse error.  Checked on the host, before any device work."""
+    def model(n):
+        return "targets, factors\n" + "".join(f"v{i}, !v{i}\n" for i in range(n))
+
+    assert esl.Model.parse(model(30)).n == 30
+    with pytest.raises(esl.EslError) as e:
+        esl.Model.parse(model(31))
+    assert e.value.code == -7 and "more than 30 nodes" in str(e.value)
+    with pytest.raises(esl.EslError) as e:
+        esl.Model.parse("targets, factors\n")
+    assert e.value.code == -2
+    # the allocation-free table build rejects more than 20 nodes before touching a device
+    m = esl.Model.parse(model(21))
+    nnz = C.c_int64(-1)
+    st = esl.lib().esl_table_build_static(m._h, np.ones(42).ctypes.data, None, C.c_void_p(1), C.c_void_p(1),
+                                          None, 0, C.byref(nnz))
+    assert st == -7 and "at most 20 nodes" in esl.lib().esl_last_error().decode()
