@@ -407,11 +407,21 @@ class Mlp:
         check(lib().esl_mlp_set_params(self._h, _ptr(p), float(mu), float(sigma)))
 
     def _samples(self, rates, ks, vs):
+        """Device copies of a sample list.  The library reads the rate-set and state
+        indices on the device without bounds checks, so they are checked here."""
         torch = _torch()
         dev = self._dev()
         rates = torch.as_tensor(rates, dtype=torch.float64, device=dev).contiguous()
         ks = torch.as_tensor(ks, dtype=torch.int32, device=dev).contiguous()
         vs = torch.as_tensor(vs, dtype=torch.int32, device=dev).contiguous()
+        if ks.numel() != vs.numel():
+            raise ValueError(f"{ks.numel()} rate-set indices but {vs.numel()} states")
+        sets = rates.numel() // (2 * self.net.n)
+        if ks.numel():
+            if int(ks.min()) < 0 or int(ks.max()) >= sets:
+                raise ValueError(f"rate-set index outside [0, {sets})")
+            if int(vs.min()) < 0 or int(vs.max()) >= self.net.N:
+                raise ValueError(f"state outside [0, {self.net.N})")
         return rates, ks, vs
 
     def features(self, rates, ks, vs):
