@@ -905,18 +905,25 @@ int eo_solve_many(const eo_sym* s, int B, const double* rates, const double* x0,
 }
 
 // Initial state as in cuda/src/initial_state.cu:7-60: uniform, or p/|F| on the
-// states matching the fixed (node, value) pairs and (1-p)/(N-|F|) elsewhere.
+// states matching the fixed (node, value) pairs and (1-p)/(N-|F|) elsewhere.  The
+// reference forms the fixed pattern as a sum of (1 << node) * value (:41-42), so a node
+// listed twice with values 1 and 0 is fixed to 1; the same node listed twice with 1
+// carries into the next bit there, which is not reproduced (bit set once).
 int eo_initial_state(int n, int n_fixed, const int32_t* nodes, const int32_t* values, double p, double* x0) {
     uint64_t N = 1ull << n;
     if (n_fixed == 0) {
         for (uint64_t s = 0; s < N; s++) x0[s] = 1.0 / (double)N;
         return 0;
     }
+    uint64_t mask = 0, val = 0;
+    for (int k = 0; k < n_fixed; k++) {
+        mask |= 1ull << nodes[k];
+        if (values[k]) val |= 1ull << nodes[k];
+    }
     uint64_t match = 0;
     std::vector<char> m(N, 1);
     for (uint64_t s = 0; s < N; s++) {
-        for (int k = 0; k < n_fixed; k++)
-            if ((int)((s >> nodes[k]) & 1) != (values[k] ? 1 : 0)) { m[s] = 0; break; }
+        m[s] = (s & mask) == val;
         match += m[s];
     }
     for (uint64_t s = 0; s < N; s++)

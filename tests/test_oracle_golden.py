@@ -36,6 +36,16 @@ def test_initial_value_toy(goldens):
     assert m.initial_state(c["fixed"], c["values"]).tolist() == c["state"]
 
 
+def test_initial_state_with_a_node_listed_twice(goldens):
+    # the reference sums (1 << node) * value: A listed with 1 and with 0 is fixed to 1
+    m = _model(goldens, "toy.bnet")
+    a = m.names[0]
+    once = m.initial_state([a], [1], p=0.8)
+    assert np.array_equal(m.initial_state([a, a], [1, 0], p=0.8), once)
+    assert np.array_equal(m.initial_state([a, a], [0, 1], p=0.8), once)
+    assert abs(once.sum() - 1.0) < 1e-15 and np.all(np.isfinite(once))
+
+
 @pytest.mark.parametrize("name", ["solver.toy", "solver.toy2", "solver.toy3"])
 def test_solver_toys(goldens, name):
     c = goldens["cases"][name]
