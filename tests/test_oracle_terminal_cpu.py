@@ -8,6 +8,7 @@
 - Per-node rates (some zero) and non-uniform x0 on small networks: the limit of the
   uniformized chain by repeated squaring."""
 import numpy as np
+import pytest
 
 import oracle as O
 from paraexastolog_b200 import synth
@@ -127,3 +128,23 @@ def test_oracle_matches_the_uniformized_limit_with_rates():
         x, _ = m.analyse(rates).solve(x0, rates)
         exact = _limit(np.asarray(m.flip_masks(rates)), rates, x0)
         assert np.abs(x - exact).sum() <= 1e-10
+
+
+@pytest.mark.parametrize("family", ["nested_canalizing", "precision"])
+def test_oracle_matches_the_uniformized_limit_on_workload_families(family):
+    # the two other generators behind the workloads, at small n: nested-canalizing
+    # rules (the drop-in workload) and Bernoulli(0.3) tables with self-holding source
+    # nodes (the precision and learned workloads: several attractors, cyclic ones too)
+    rng = np.random.default_rng(12 if family == "precision" else 13)
+    for seed in range(8):
+        n = int(rng.integers(6, 9))
+        if family == "precision":
+            net = synth.precision_network(seed, n)
+        else:
+            net = synth.nested_canalizing_network(rng, n, 3)
+        rates = synth.log_uniform_rates(rng, n, 1)[0]
+        x0 = synth.dirichlet_subspace_x0(rng, n, rng.choice(n, 3, replace=False))
+        m = O.Model(text=net.bnet)
+        x, _ = m.analyse(rates).solve(x0, rates)
+        exact = _limit(np.asarray(m.flip_masks(rates)), rates, x0)
+        assert np.abs(x - exact).sum() <= 1e-10, (family, seed)
