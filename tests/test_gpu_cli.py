@@ -153,6 +153,6 @@ def test_cli_turns_away_a_damaged_symbolic_file(esl, cli, goldens, tmp_path):
     symb.write_bytes(bytes(bad))
     assert _run(cli, path, "-s") == plain
     sizes2, arrays2 = _read_symb(symb)
-    assert sizes2 == sizes
+    assert sizes2[:7] == sizes[:7]
     for k in range(7):  # table, order, SCC offsets and rates as first written
         assert np.array_equal(arrays2[k], arrays[k]), k
