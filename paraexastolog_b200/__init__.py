@@ -482,6 +482,32 @@ class SolveResult:
     status: int = 0
 
 
+def _check_batch(n: int, rates, x0, warm=None, occupation=None, out=None, device=None):
+    """(B, R) of a batch of B rate sets (B x 2n) and R initial distributions (R x 2^n),
+    or ValueError.  The library reads and writes every buffer by the sizes the network
+    implies, so a short or mistyped one would be read or written past its end; the
+    device buffers must also live on the context's device (``device``, if given)."""
+    N = 1 << n
+    if rates.dim() != 2 or rates.shape[1] != 2 * n or rates.shape[0] < 1:
+        raise ValueError(f"rates must be B x {2 * n} (B >= 1), got {tuple(rates.shape)}")
+    if x0.dim() != 2 or x0.shape[1] != N or x0.shape[0] < 1:
+        raise ValueError(f"x0 must be R x {N} (R >= 1), got {tuple(x0.shape)}")
+    B, R = rates.shape[0], x0.shape[0]
+    for name, t, shape in (("warm", warm, None), ("occupation", occupation, None), ("out", out, (B, R, N))):
+        if t is None:
+            continue
+        import torch
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float64 or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous float64 tensor")
+        if shape is not None and tuple(t.shape) != shape:
+            raise ValueError(f"{name} must be {shape}, got {tuple(t.shape)}")
+        if t.numel() != B * R * N:
+            raise ValueError(f"{name} must hold {B} x {R} x {N} values, got {t.numel()}")
+        if device is not None and (not t.is_cuda or t.device.index != device):
+            raise ValueError(f"{name} must be on cuda:{device}")
+    return B, R
+
+
 def _opts(method: int, tol: float, max_iters: int, max_refine: int, warm=None, occupation=None) -> SolveOpts:
     return SolveOpts(method, tol, max_iters, max_refine, _ptr(warm), _ptr(occupation))
 
@@ -495,6 +521,7 @@ def solve(ctx: Context, net: Net, rates, x0, want_R: bool = False, want_L: bool 
     rates = torch.as_tensor(np.ascontiguousarray(rates, np.float64) if isinstance(rates, np.ndarray) else rates,
                             dtype=torch.float64, device=dev).contiguous()
     x0 = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
+    _check_batch(net.n, rates.reshape(1, -1), x0.reshape(1, -1))
     xi = torch.empty(net.N, dtype=torch.float64, device=dev)
     mg = torch.empty(net.n, dtype=torch.float64, device=dev)
     Rv = torch.empty(max(net.terminal_states, 1), dtype=torch.float64, device=dev) if want_R else None
@@ -521,7 +548,7 @@ def solve_batch(ctx: Context, net: Net, rates, x0, method: int = METHOD_FP64, to
         rates = rates[None]
     if x0.dim() == 1:
         x0 = x0[None]
-    B, R = rates.shape[0], x0.shape[0]
+    B, R = _check_batch(net.n, rates, x0, warm, occupation, out, ctx.device)
     xi = out if out is not None else torch.empty((B, R, net.N), dtype=torch.float64, device=dev)
     mg = torch.empty((B, R, net.n), dtype=torch.float64, device=dev) if marginals else None
     rep = Report()
@@ -545,7 +572,7 @@ def solve_many(ctxs: Sequence[Context], jobs, method: int = METHOD_DIRECT, tol: 
         x = torch.as_tensor(x0, dtype=torch.float64, device=dev).contiguous()
         r = r[None] if r.dim() == 1 else r
         x = x[None] if x.dim() == 1 else x
-        B, R = r.shape[0], x.shape[0]
+        B, R = _check_batch(net.n, r, x)
         xi = torch.empty((B, R, net.N), dtype=torch.float64, device=dev)
         mg = torch.empty((B, R, net.n), dtype=torch.float64, device=dev)
         keep += [r, x]
@@ -569,7 +596,8 @@ def solve_host(ctx: Context, model: Model, rates: np.ndarray, x0: np.ndarray, me
     """Host arrays in, host arrays out (builds its own symbolic data)."""
     rates = np.ascontiguousarray(np.atleast_2d(rates), np.float64)
     x0 = np.ascontiguousarray(np.atleast_2d(x0), np.float64)
-    B, R = rates.shape[0], x0.shape[0]
+    torch = _torch()
+    B, R = _check_batch(model.n, torch.from_numpy(rates), torch.from_numpy(x0))
     N = 1 << model.n
     xi = np.zeros((B, R, N))
     mg = np.zeros((B, R, model.n))

@@ -242,3 +242,36 @@ def test_node_count_limits():
     st = esl.lib().esl_table_build_static(m._h, np.ones(42).ctypes.data, None, C.c_void_p(1), C.c_void_p(1),
                                           None, 0, C.byref(nnz))
     assert st == -7 and "at most 20 nodes" in esl.lib().esl_last_error().decode()
+
+
+def test_batch_buffers_are_checked_before_the_library_sees_them():
+    """The library reads and writes every batch buffer by the sizes the network implies:
+    a short, mistyped or misplaced one is a ValueError in the binding, not an access past
+    its end."""
+    import torch
+
+    n, N = 4, 16
+    r, x = torch.ones(3, 2 * n, dtype=torch.float64), torch.full((2, N), 1.0 / N, dtype=torch.float64)
+    assert esl._check_batch(n, r, x) == (3, 2)
+    assert esl._check_batch(n, r, x, warm=torch.zeros(6, N, dtype=torch.float64),
+                            occupation=torch.zeros(6 * N, dtype=torch.float64),
+                            out=torch.zeros(3, 2, N, dtype=torch.float64)) == (3, 2)
+    bad = [
+        dict(rates=torch.ones(3, 2 * n + 1, dtype=torch.float64)),    # wrong rate width
+        dict(x0=torch.ones(2, N - 1, dtype=torch.float64)),           # short x0 rows
+        dict(x0=torch.ones(2, 2, N, dtype=torch.float64)),            # x0 not R x N
+        dict(warm=torch.zeros(5, N, dtype=torch.float64)),            # one system short
+        dict(occupation=torch.zeros(6, N, dtype=torch.float32)),      # float32: half the bytes
+        dict(occupation=torch.zeros(N, 6, dtype=torch.float64).t()),  # not contiguous
+        dict(out=torch.zeros(2, 3, N, dtype=torch.float64)),          # B and R swapped
+        dict(warm=np.zeros((6, N))),                                  # not a tensor
+    ]
+    for kw in bad:
+        args = dict(rates=r, x0=x)
+        args.update(kw)
+        with pytest.raises(ValueError):
+            esl._check_batch(n, args.pop("rates"), args.pop("x0"), **args)
+    # device buffers must be on the context's device: a host tensor's address is no
+    # device address
+    with pytest.raises(ValueError, match="cuda:0"):
+        esl._check_batch(n, r, x, warm=torch.zeros(6, N, dtype=torch.float64), device=0)
