@@ -355,10 +355,13 @@ def run_reference(args):
         solves += sample
     value = solves / total
     cb["value"] = value
-    return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+    # n_gpus is the N this arm was launched with (so that it pairs with our arm's line);
+    # the work itself runs on the host cores of rank 0 only
+    return {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "sample_per_step": sample},
+            "config": {"workload": "n20_precision_network_x_512_heldout_rate_sets", "sample_per_step": sample,
+                       "device": "host cores of rank 0 (no GPU)"},
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
