@@ -1,4 +1,5 @@
-"""The oracle's graph stages against an independent computation: strongly connected
+"""The oracle's table and graph stages against independent computations.  The table:
+from the generator's truth tables, without the bnet text.  The graph: strongly connected
 components from scipy (scipy.sparse.csgraph), terminal SCCs as the sinks of the
 condensation, and levels by a longest-path recursion over the condensation (level 1 =
 terminal, otherwise 1 + the largest level of a successor SCC).  The reference's own
@@ -86,3 +87,40 @@ def test_graph_stages_match_scipy(family):
         assert np.all(lev_at[: sym.T] == 1) and np.all(lev_at[sym.T:] > 1)
         assert np.all(np.diff(lev_at[sym.T:]) <= 0)
         assert sym.T == int(np.sum(level == 1))
+
+
+@pytest.mark.parametrize("family", ["table", "nested_canalizing", "precision"])
+def test_table_matches_the_truth_tables(family):
+    # the transition table from the generator's truth tables alone (no bnet text, no
+    # DNF): node i flips in state s iff its rule disagrees with bit i and the rate of
+    # that direction is not zero; the CSC lists each source's destinations ascending
+    rng = np.random.default_rng({"table": 31, "nested_canalizing": 32, "precision": 33}[family])
+    for seed in range(6):
+        n = int(rng.integers(6, 12))
+        if family == "table":
+            net = synth.random_table_network(rng, n, [1, 2, 3, 4], 0.5)
+        elif family == "nested_canalizing":
+            net = synth.nested_canalizing_network(rng, n, 3)
+        else:
+            net = synth.precision_network(seed, n)
+        rates = synth.log_uniform_rates(rng, n, 1)[0]
+        rates[rng.choice(2 * n, 3, replace=False)] = 0.0
+        N = 1 << n
+        s = np.arange(N, dtype=np.int64)
+        F = np.zeros(N, np.int64)
+        for i in range(n):
+            idx = np.zeros(N, np.int64)
+            for j, inp in enumerate(net.inputs[i]):
+                idx |= ((s >> inp) & 1) << j
+            f = np.asarray(net.tables[i], bool)[idx]
+            bit = ((s >> i) & 1).astype(bool)
+            rate_ok = np.where(bit, rates[2 * i + 1] != 0.0, rates[2 * i] != 0.0)
+            F |= ((f != bit) & rate_ok).astype(np.int64) << i
+        m = O.Model(text=net.bnet)
+        assert np.array_equal(np.asarray(m.flip_masks(rates)).astype(np.int64), F), (family, seed)
+        indptr, rows, cols = m.table(rates)
+        deg = np.array([bin(int(v)).count("1") for v in F])
+        assert np.array_equal(np.diff(indptr), deg)
+        expect_rows = np.concatenate([np.sort(v ^ (1 << np.nonzero((F[v] >> np.arange(n)) & 1)[0]))
+                                      for v in range(N)])
+        assert np.array_equal(rows, expect_rows) and np.array_equal(cols, np.repeat(np.arange(N), deg))
