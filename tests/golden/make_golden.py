@@ -13,13 +13,18 @@ Contents:
   initial state and the expected arrays, parsed from the test source.
 * ``python_ref``: x_inf produced by the reference's Python CPU implementation
   (``python/exastolog.py``) for uniform-rate networks: the small-database
-  models and the seeded n=10 network, run through a shim because its optional
+  models, the seeded n=10 network and 24 seeded random networks (n = 6-10, terminal
+  SCCs of at most 64 states), run through a shim because its optional
   dependencies (pyeda, sortednp, scikit-umfpack) are absent; models above 12
   nodes are skipped (its terminal kernels densify whole attractors).  The Python path
   ignores per-node rates (``exastolog.py:328-331``) and mis-places terminal
   kernels when a weak component holds a cyclic attractor followed by another
-  attractor (``exastolog.py:365-375``); cases whose x_inf does not sum to 1 are
-  recorded with ``"valid": false`` and skipped by the tests.
+  attractor (``exastolog.py:365-375``).  A result is recorded ``"valid": true`` only
+  if it sums to 1 and matches the uniformized limit below to L1 1e-9; the others
+  (a run that raises included) are recorded with ``"valid": false`` and skipped.
+* ``uniformized_limits``: for every model above, lim exp(K t) x0 (uniform rates and
+  x0) by repeated squaring of the uniformized chain: an exact answer that depends on
+  the transition table alone (``uniformized_limit``).
 """
 from __future__ import annotations
 
