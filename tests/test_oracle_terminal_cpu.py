@@ -94,8 +94,8 @@ def test_large_transient_block_closed_form():
     np.testing.assert_allclose(marg[2:], 0.5, rtol=0, atol=1e-11)
 
 
-def _limit(F, rates, x0):
-    """lim exp(K t) x0 by repeated squaring of the uniformized chain (columns renormalised);
+def _limit_matrix(F, rates):
+    """lim exp(K t) by repeated squaring of the uniformized chain (columns renormalised);
     uses the transition table only."""
     n = int(np.log2(F.size))
     N = F.size
@@ -111,7 +111,11 @@ def _limit(F, rates, x0):
     for _ in range(80):
         P = P @ P
         P /= P.sum(0, keepdims=True)
-    return P @ x0
+    return P
+
+
+def _limit(F, rates, x0):
+    return _limit_matrix(F, rates) @ x0
 
 
 def test_oracle_matches_the_uniformized_limit_with_rates():
@@ -148,3 +152,21 @@ def test_oracle_matches_the_uniformized_limit_on_workload_families(family):
         x, _ = m.analyse(rates).solve(x0, rates)
         exact = _limit(np.asarray(m.flip_masks(rates)), rates, x0)
         assert np.abs(x - exact).sum() <= 1e-10, (family, seed)
+
+
+def test_absorption_matrix_matches_the_limit_matrix():
+    # L[t, s]: the probability of ending in terminal SCC t from state s, which is the
+    # mass the limit matrix moves from s onto t's states (backward formulation)
+    rng = np.random.default_rng(17)
+    for _ in range(8):
+        n = int(rng.integers(5, 9))
+        net = synth.random_table_network(rng, n, [1, 2, 3], 0.5)
+        rates = synth.log_uniform_rates(rng, n, 1)[0]
+        m = O.Model(text=net.bnet)
+        sym = m.analyse(rates)
+        Lm = sym.absorption(rates)
+        P = _limit_matrix(np.asarray(m.flip_masks(rates)), rates)
+        order, offs = np.asarray(sym.order), np.asarray(sym.offsets)
+        expect = np.stack([P[order[offs[t]:offs[t + 1]]].sum(0) for t in range(sym.T)])
+        assert np.abs(Lm - expect).max() <= 1e-10
+        np.testing.assert_allclose(Lm.sum(0), 1.0, rtol=0, atol=1e-11)
