@@ -345,7 +345,9 @@ def cpu_baseline(sample: int):
 
 
 def run_reference(args):
-    sample = max(8, min(os.cpu_count() or 8, 32))
+    # one rate set per host thread, up to 128 threads (~60 MB each): a step takes about
+    # one oracle solve (~35 s) however many threads run
+    sample = max(8, min(os.cpu_count() or 8, 128))
     for _ in range(min(args.warmup, 1)):
         cpu_baseline(sample)
     total, solves = 0.0, 0
