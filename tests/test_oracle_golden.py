@@ -157,3 +157,19 @@ def test_bnet_quirks():
     assert pos[off[0]:off[1]].tolist() == [2]
     with pytest.raises(O.OracleError):
         O.Model(text="targets, factors\nA, (A & \nB, B\n")
+
+
+def test_threaded_solve_many_equals_serial_solves():
+    # the CPU baseline and several GPU tests use the oracle's threaded batch solve
+    from paraexastolog_b200 import synth
+
+    rng = np.random.default_rng(9)
+    net = synth.random_table_network(rng, 10, [2, 3], 0.5)
+    rates = synth.log_uniform_rates(rng, 10, 6)
+    x0 = np.stack([synth.dirichlet_subspace_x0(rng, 10, rng.choice(10, 4, replace=False)) for _ in range(6)])
+    s = O.Model(text=net.bnet).analyse(rates[0])
+    many, marg = s.solve_many(rates, x0, threads=4)
+    for k in range(6):
+        one, om = s.solve(x0[k], rates[k])
+        assert np.array_equal(many.reshape(6, -1)[k], one)
+        assert np.array_equal(marg.reshape(6, -1)[k], om)
