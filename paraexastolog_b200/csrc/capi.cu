@@ -558,15 +558,19 @@ int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates,
     if (st == ESL_OK) st = dxi.alloc((size_t)B * R * N);
     if (st == ESL_OK && marginals) st = dm.alloc((size_t)B * R * n);
     if (st == ESL_OK) {
-        cudaMemcpyAsync(dr.get(), rates, (size_t)B * 2 * n * 8, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dx0.get(), x0, (size_t)R * N * 8, cudaMemcpyHostToDevice, s);
-        st = esl_solve_batch(ctx, net, B, dr.get(), R, dx0.get(), dxi.get(), marginals ? dm.get() : nullptr, opts,
-                             report);
+        if (cudaMemcpyAsync(dr.get(), rates, (size_t)B * 2 * n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(dx0.get(), x0, (size_t)R * N * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            st = fail(ESL_ERR_CUDA, "copy to the device failed");
+        else
+            st = esl_solve_batch(ctx, net, B, dr.get(), R, dx0.get(), dxi.get(), marginals ? dm.get() : nullptr,
+                                 opts, report);
     }
     if (st == ESL_OK) {
-        cudaMemcpyAsync(x_inf, dxi.get(), (size_t)B * R * N * 8, cudaMemcpyDeviceToHost, s);
-        if (marginals) cudaMemcpyAsync(marginals, dm.get(), (size_t)B * R * n * 8, cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(ESL_ERR_CUDA, "copy back failed");
+        if (cudaMemcpyAsync(x_inf, dxi.get(), (size_t)B * R * N * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            (marginals &&
+             cudaMemcpyAsync(marginals, dm.get(), (size_t)B * R * n * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            st = fail(ESL_ERR_CUDA, "copy back failed");
     }
     esl_net_free(net);
     return st;
