@@ -36,7 +36,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-from paraexastolog_b200 import synth  # noqa: E402
+from paraexastolog_b200 import shards, synth  # noqa: E402
 
 METRIC = "solves/s, n=20 x 512 rate sets, learned+mixed vs FP64 sparse LU at L1<=1e-9"
 BATCH = 512
@@ -45,16 +45,20 @@ BATCH = 512
 N_TRAIN = 3584
 
 
-def workload(rank: int):
-    """(network, held-out rate sets of this rank, x0, training rate sets)."""
+def workload(rank: int = 0, world: int = 1):
+    """(network, this rank's rate sets, x0, training rate sets, [begin, end) of the
+    rank's slice of the global sweep).  Weak scaling: the global sweep is the 512
+    held-out rate sets followed, for world > 1, by further seeded log-uniform draws
+    (shards.global_sweep); rank r solves its shard_bounds slice, BATCH rate sets."""
     w = synth.config_learned(n_rate_sets=4096)
     net = w.networks[0]
-    rates = w.rates[0][-BATCH:]
-    if rank > 0:  # weak scaling: further seeded rate sets of the same distribution
-        rng = np.random.default_rng(10_000 + rank)
-        rates = synth.log_uniform_rates(rng, net.n, BATCH)
-    return (net, np.ascontiguousarray(rates), np.ascontiguousarray(w.x0[0]),
-            np.ascontiguousarray(w.rates[0][:N_TRAIN]))
+    held = np.ascontiguousarray(w.rates[0][-BATCH:])
+
+    def draw(seed, count):
+        return synth.log_uniform_rates(np.random.default_rng(10_000 + seed), net.n, count)
+
+    rates, bounds = shards.rank_rate_sets(held, rank, world, draw)
+    return (net, rates, np.ascontiguousarray(w.x0[0]), np.ascontiguousarray(w.rates[0][:N_TRAIN]), bounds)
 
 
 def train_warm_start(esl, torch, ctx, net, x0, train_rates, steps: int, device: int):
@@ -142,6 +146,45 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def kernel_rooflines(entries):
+    """Per kernel class of one profiled step: launches, device ms, algorithmic bytes
+    and GB/s.  For the Schur operator and the BiCGStab updates, records of the largest
+    level group (at least half the class's largest per-launch bytes) are listed apart."""
+    out = []
+    classes = sorted({e[0] for e in entries})
+    for name in classes:
+        rec = [e for e in entries if e[0] == name]
+        groups = [("all", rec)]
+        if name in ("schur_operator", "bicgstab_update"):
+            cut = 0.5 * max(e[2] for e in rec)
+            groups.append(("largest_level_group", [e for e in rec if e[2] >= cut]))
+        for scope, rr in groups:
+            ms = sum(e[1] for e in rr)
+            by = sum(e[2] for e in rr)
+            out.append({"kernel": name, "scope": scope, "launches": len(rr), "ms": ms,
+                        "bytes_per_launch": by / len(rr), "achieved": by / (ms * 1e-3) / 1e9 if ms > 0 else None,
+                        "unit": "GB/s"})
+    return out
+
+
+def table_rooflines(esl, torch, ctx, model, rates, label, repeats: int = 5):
+    """k_flip_masks (out-masks only) and k_emit_csc of esl_table_build, best of
+    `repeats` builds (the first one untimed)."""
+    esl.table(ctx, model, rates, with_cols=False)
+    best = {}
+    for _ in range(repeats):
+        ctx.set_profiling(True)
+        esl.table(ctx, model, rates, with_cols=False)
+        for name, ms, by in ctx.profile_entries():
+            if name not in best or ms < best[name][0]:
+                best[name] = (ms, by)
+        ctx.set_profiling(False)
+    torch.cuda.synchronize()
+    return [{"kernel": name, "scope": label, "launches": 1, "ms": ms, "bytes_per_launch": by,
+             "achieved": by / (ms * 1e-3) / 1e9 if ms > 0 else None, "unit": "GB/s", "timing": "best of 5"}
+            for name, (ms, by) in sorted(best.items())]
+
+
 def run_ours(args, rank, world, device):
     import torch
     import torch.distributed as dist
@@ -154,7 +197,7 @@ def run_ours(args, rank, world, device):
     stream = torch.cuda.Stream(device)
     torch.cuda.set_stream(stream)
     ctx = esl.Context(device, stream)
-    net_g, rates, x0, train_rates = workload(rank)
+    net_g, rates, x0, train_rates, bounds = workload(rank, world)
     model = esl.Model.parse(net_g.bnet)
     d_rates = torch.tensor(rates, device=f"cuda:{device}")
     d_x0 = torch.tensor(x0, device=f"cuda:{device}")
@@ -230,16 +273,25 @@ def run_ours(args, rank, world, device):
             other["warm_start_inference_ms"] = pms / 3
             other["warm_start_training"] = train_info
 
-    # roofline of the dominant kernel pair (Schur operator) from live CUDA events
+    # rooflines from live CUDA events on the library's stream: every hot kernel class of
+    # one step (table masks, graph sweeps, Schur operator, BiCGStab updates), and the CSC
+    # emission of the transition table of this network and of the n=22 drop-in network
     ctx.set_profiling(True)
-    for _ in range(max(1, min(args.steps, 2))):
-        step()
-    op_ms, op_bytes, op_launches = ctx.profile()
-    rec_ms, rec_bytes = ctx.profile_records()
+    step()
+    entries = ctx.profile_entries()
     ctx.set_profiling(False)
+    kernels = kernel_rooflines(entries)
+    kernels += table_rooflines(esl, torch, ctx, model, rates[0], "n20_bench_network")
+    scale = synth.config_scale()
+    m22 = esl.Model.parse(scale.networks[0].bnet)
+    kernels += table_rooflines(esl, torch, ctx, m22, scale.rates[0][0], "n22_drop_in_network")
+    del m22
+    op = [e for e in entries if e[0] == "schur_operator"]
+    op_ms, op_bytes = sum(e[1] for e in op), sum(e[2] for e in op)
     # the applications of the largest level group (the one that dominates the step)
-    big = rec_bytes >= 0.5 * rec_bytes.max() if rec_bytes.size else rec_bytes.astype(bool)
-    big_ms, big_bytes, big_n = float(rec_ms[big].sum()), float(rec_bytes[big].sum()), int(big.sum())
+    big_cut = 0.5 * max((e[2] for e in op), default=0.0)
+    big = [e for e in op if e[2] >= big_cut]
+    big_ms, big_bytes, big_n = sum(e[1] for e in big), sum(e[2] for e in big), len(big)
 
     # end to end through the public API: pinned host inputs, results back to host
     h_rates = torch.tensor(rates).pin_memory()
@@ -266,14 +318,14 @@ def run_ours(args, rank, world, device):
     e2e_ms = f0.elapsed_time(f1)
     e2e_wall = time.perf_counter() - t_wall
 
-    t = torch.tensor([ms, e2e_ms, float(launches)], device=f"cuda:{device}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = shards.max_over_ranks([ms, e2e_ms], world, device=f"cuda:{device}")
     out = None
     if rank == 0:
         solves = BATCH * args.steps * world
         peak, peak_kind = peaks()
+        for k in kernels:
+            k["peak"] = peak
+            k["frac"] = k["achieved"] / peak if k.get("achieved") else None
         achieved_all = op_bytes / (op_ms * 1e-3) / 1e9 if op_ms > 0 else None
         achieved = big_bytes / (big_ms * 1e-3) / 1e9 if big_ms > 0 else None
         tpb = traffic_per_byte()
@@ -296,6 +348,10 @@ def run_ours(args, rank, world, device):
                        "method": "learned+mixed" if learned else args.method, "tol_relres": args.tol,
                        "l2": "working set > L2 (x_inf alone is 4 GB per step)",
                        "parallelism": f"replicas x{world} (rate-set shards)",
+                       "sweep": f"rank 0 solves rate sets [{bounds[0]}, {bounds[1]}) of a {BATCH * world}-set "
+                                "global sweep (the 512 held-out sets, then seeded draws for world > 1)",
+                       "denominator": "the plain FP64 form is a level sweep of FP64 BiCGStab on the odd-row "
+                                      "Schur complement of each level group (no sparse LU factorisation)",
                        "step": ("table + SCC/levels/order + terminal kernels + " +
                                 ("warm-start inference + " if learned else "") +
                                 "transient solve + x_inf/marginals")},
@@ -312,9 +368,10 @@ def run_ours(args, rank, world, device):
                          "launches": big_n,
                          "all_groups": {"achieved": achieved_all,
                                         "frac": achieved_all / peak if achieved_all else None,
-                                        "launches": op_launches,
+                                        "launches": len(op),
                                         "note": "first poll window of every Krylov group; small groups "
-                                                "are launch-latency bound"}},
+                                                "are launch-latency bound"},
+                         "kernels": kernels},
             "solver": {"iterations": iters, "relres": relres},
             "clocks": clocks,
         }
@@ -326,15 +383,15 @@ def run_ours(args, rank, world, device):
     return out, last_xinf
 
 
-def cpu_baseline(sample: int):
-    """The CPU FP64 oracle on this host's cores over a bounded sample of rate sets;
-    returns (baseline record, seconds, the oracle's x_inf of the sample)."""
+def cpu_baseline(sample: int, rank: int = 0, world: int = 1, threads: int = 0):
+    """The CPU FP64 oracle on this host's cores over a bounded sample of the rank's rate
+    sets; returns (baseline record, seconds, the oracle's x_inf of the sample)."""
     import oracle as O
 
-    net_g, rates, x0, _ = workload(0)
+    net_g, rates, x0, _, _ = workload(rank, world)
     m = O.Model(text=net_g.bnet)
     sym = m.analyse(rates[0])
-    threads = min(os.cpu_count() or 1, sample)
+    threads = threads or min(os.cpu_count() or 1, sample)
     r = rates[:sample]
     xs = np.broadcast_to(x0, (sample, x0.size)).copy()
     t = time.perf_counter()
@@ -387,11 +444,26 @@ def main():
     ap.add_argument("--batch", type=int, default=BATCH, help="held-out rate sets per step (profiling of smaller cases)")
     ap.add_argument("--profile-run", action="store_true",
                     help="run --warmup steps and then exactly one step, nothing else (for ncu launch lists)")
+    ap.add_argument("--profile-table", action="store_true",
+                    help="build the CSC transition tables of the n=20 bench network and of the n=22 drop-in "
+                         "network once each, nothing else (for ncu captures of the table kernels)")
     args = ap.parse_args()
     BATCH = args.batch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.profile_table:
+        import torch
+
+        import paraexastolog_b200 as esl
+        ctx = esl.Context(local)
+        net_g, rates, _, _, _ = workload(0, 1)
+        scale = synth.config_scale()
+        for text, r in ((net_g.bnet, rates[0]), (scale.networks[0].bnet, scale.rates[0][0])):
+            esl.table(ctx, esl.Model.parse(text), r, with_cols=False)
+        torch.cuda.synchronize()
+        return
 
     if args.impl == "reference":
         if rank == 0:
@@ -408,15 +480,24 @@ def main():
     out, xinf = run_ours(args, rank, world, local)
     if args.profile_run:
         return
-    if rank == 0:
-        if not args.no_cpu_baseline and world == 1:
+    if not args.no_cpu_baseline:
+        # error of this run's results against the FP64 oracle on a sample of every rank's
+        # rate sets; at N=1 the same oracle run is the timed CPU baseline
+        if world == 1:
             sample = max(8, min(os.cpu_count() or 8, 16))
-            out["cpu_baseline"], _, ref = cpu_baseline(sample)
-            # error of this run's results against the FP64 oracle on the sampled rate sets
-            got = xinf[:sample, 0].cpu().numpy()
-            diff = np.abs(got - ref.reshape(sample, -1))
-            out["accuracy_vs_fp64_oracle"] = {"rate_sets": sample, "l1_max": float(diff.sum(1).max()),
-                                              "maxabs": float(diff.max()), "target_l1": 1e-9}
+            cb, _, ref = cpu_baseline(sample)
+        else:
+            sample = 2
+            cb, _, ref = cpu_baseline(sample, rank, world, threads=max(1, (os.cpu_count() or 2) // world))
+        got = xinf[:sample, 0].cpu().numpy()
+        diff = np.abs(got - ref.reshape(sample, -1))
+        l1, mx = shards.max_over_ranks([diff.sum(1).max(), diff.max()], world, device=f"cuda:{local}")
+        if rank == 0:
+            if world == 1:
+                out["cpu_baseline"] = cb
+            out["accuracy_vs_fp64_oracle"] = {"rate_sets": sample * world, "l1_max": l1, "maxabs": mx,
+                                              "target_l1": 1e-9, "ranks": world}
+    if rank == 0:
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

@@ -124,7 +124,9 @@ int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32
  *      always receives the edge count once it is known, and a table with more than
  *      rows_capacity edges returns ESL_ERR_TOO_LARGE without writing the arrays.
  *      The first call on a device looks up the array's device address; make that
- *      first call before any stream capture.  All calls on a device share the
+ *      first call before any stream capture.  The address is kept for the life of
+ *      the process: after cudaDeviceReset on a device, do not call this entry point
+ *      on that device again.  All calls on a device share the
  *      array: calls whose GPU work overlaps race, so serialise them.
  *      Synchronises the stream before returning. */
 #define ESL_STATIC_TABLE_MAX_NODES 20
@@ -239,15 +241,22 @@ int esl_mlp_train(esl_mlp* mlp, int B, const double* d_rates, const double* d_oc
 /* warm start d_warm (B x N, device) for B rate sets: predicted occupation on the targets, 0 elsewhere */
 int esl_mlp_predict(esl_mlp* mlp, int B, const double* d_rates, double* d_warm);
 
-/* ---- measurement hook (no counterpart in the reference): when on, the solver
- *      records CUDA events around every application of the reduced (Schur) operator
- *      in its Krylov loop.  esl_ctx_profile returns the summed device time, the
- *      algorithmic bytes (each array touched once per launch) and the launch count
- *      since profiling was switched on. */
+/* ---- measurement hook (no counterpart in the reference): when on, the library
+ *      records CUDA events around the launches of its hot kernels (table, graph sweeps,
+ *      every application of the reduced (Schur) operator and the BiCGStab vector updates
+ *      of the first convergence-poll window of each Krylov group).  esl_ctx_profile
+ *      returns the summed device time, the algorithmic bytes (each array touched once per
+ *      launch) and the record count since profiling was switched on. */
 int esl_ctx_set_profiling(esl_ctx* ctx, int on);
 int esl_ctx_profile(esl_ctx* ctx, double* total_ms, double* total_bytes, int* launches);
 /* the same per recorded application: *count records, the first `cap` written */
 int esl_ctx_profile_records(esl_ctx* ctx, int cap, double* ms, double* bytes, int* count);
+/* record i (0 <= i < count): its kernel class ("k_flip_masks", "k_emit_csc", "graph_sweep",
+ * "schur_operator", "bicgstab_update", "schur_operator_whole_system"), device ms and
+ * algorithmic bytes.  Besides the Schur operator, profiling records the table kernels, the
+ * fixpoint sweeps of the graph stages and the BiCGStab vector updates; esl_ctx_profile and
+ * esl_ctx_profile_records cover every record. */
+int esl_ctx_profile_entry(esl_ctx* ctx, int i, const char** name, double* ms, double* bytes);
 /* number of kernels this library has launched in this process (no counterpart in the reference) */
 int esl_launch_count(uint64_t* count);
 

@@ -77,6 +77,7 @@ def lib():
     L.esl_launch_count.argtypes = [P(C.c_uint64)]
     L.esl_ctx_profile.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_int)]
     L.esl_ctx_profile_records.argtypes = [vp, C.c_int, vp, vp, P(C.c_int)]
+    L.esl_ctx_profile_entry.argtypes = [vp, C.c_int, P(cp), P(C.c_double), P(C.c_double)]
     L.esl_model_load.argtypes = [cp, P(vp)]
     L.esl_model_parse.argtypes = [cp, P(vp)]
     L.esl_model_free.argtypes = [vp]
@@ -193,8 +194,20 @@ class Context:
         check(lib().esl_ctx_profile(self._h, C.byref(ms), C.byref(by), C.byref(n)))
         return ms.value, by.value, n.value
 
+    def profile_entries(self):
+        """Every record since profiling was switched on: (kernel class, device ms,
+        algorithmic bytes) tuples in launch order."""
+        n = C.c_int()
+        check(lib().esl_ctx_profile_records(self._h, 0, None, None, C.byref(n)))
+        out = []
+        name, ms, by = C.c_char_p(), C.c_double(), C.c_double()
+        for i in range(n.value):
+            check(lib().esl_ctx_profile_entry(self._h, i, C.byref(name), C.byref(ms), C.byref(by)))
+            out.append((name.value.decode(), ms.value, by.value))
+        return out
+
     def profile_records(self):
-        """Per recorded operator application: (device ms, algorithmic bytes) arrays."""
+        """Per record: (device ms, algorithmic bytes) arrays."""
         n = C.c_int()
         check(lib().esl_ctx_profile_records(self._h, 0, None, None, C.byref(n)))
         ms = np.zeros(n.value)

@@ -73,7 +73,11 @@ int table_pass(esl_ctx* ctx, const Model& m, const double* rates, DevBuf<uint32_
     if (want_G) ESL_TRY(G.alloc(N));
     const int64_t blocks = flip_mask_blocks(m.n());
     ESL_TRY(counts.alloc(blocks + 1));
-    ESL_TRY(launch_flip_masks(dm, F.get(), want_G ? G.get() : nullptr, counts.get(), s));
+    {
+        // algorithmic bytes: the masks written (4 B per state each) and the block counts
+        ProfScope ps(ctx, "k_flip_masks", (double)N * (want_G ? 8.0 : 4.0) + 4.0 * blocks);
+        ESL_TRY(launch_flip_masks(dm, F.get(), want_G ? G.get() : nullptr, counts.get(), s));
+    }
     std::vector<uint32_t> h(blocks);
     ESL_CUDA(cudaMemcpyAsync(h.data(), counts.get(), blocks * 4, cudaMemcpyDeviceToHost, s));
     ESL_CUDA(cudaStreamSynchronize(s));
@@ -177,6 +181,18 @@ int esl_ctx_profile_records(esl_ctx* c, int cap, double* ms, double* bytes, int*
         ms[i] = t;
         bytes[i] = c->prof_recs[i].bytes;
     }
+    return ESL_OK;
+}
+
+int esl_ctx_profile_entry(esl_ctx* c, int i, const char** name, double* ms, double* bytes) {
+    if (!c || !name || !ms || !bytes) return fail(ESL_ERR_INVALID, "NULL argument");
+    if (i < 0 || i >= (int)c->prof_recs.size()) return fail(ESL_ERR_INVALID, "no such profile record");
+    ESL_CUDA(cudaStreamSynchronize(c->stream));
+    float t = 0.f;
+    ESL_CUDA(cudaEventElapsedTime(&t, c->prof_recs[i].a, c->prof_recs[i].b));
+    *name = c->prof_recs[i].name;
+    *ms = t;
+    *bytes = c->prof_recs[i].bytes;
     return ESL_OK;
 }
 
@@ -403,7 +419,13 @@ int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32
     DevBuf<uint8_t> tbuf;
     ESL_TRY(tbuf.alloc(tmp));
     ESL_CUDA(cub::DeviceScan::ExclusiveSum(tbuf.get(), tmp, counts.get(), offs.get(), (int)blocks, ctx->stream));
-    ESL_TRY(launch_emit_csc(m->m.n(), F.get(), offs.get(), d_indptr, d_rows, d_cols, nnz, ctx->stream));
+    {
+        // algorithmic bytes: the out-masks read and indptr written (4 B per state each),
+        // destinations (and sources) written (4 B per edge each)
+        const double N = (double)(1ull << m->m.n());
+        ProfScope ps(ctx, "k_emit_csc", 8.0 * N + 4.0 + (d_cols ? 8.0 : 4.0) * (double)nnz);
+        ESL_TRY(launch_emit_csc(m->m.n(), F.get(), offs.get(), d_indptr, d_rows, d_cols, nnz, ctx->stream));
+    }
     ESL_CUDA(cudaStreamSynchronize(ctx->stream));
     return ESL_OK;
 }

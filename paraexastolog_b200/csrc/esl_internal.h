@@ -121,11 +121,13 @@ struct esl_ctx {
     // level-sweep tiling of the last esl_net_autotune on this context (0 / -1: default),
     // used for networks that have no tuning of their own
     int tune_tile_mb = 0, tune_s2 = -1;
-    // measurement hook: events around Schur-operator applications
+    // measurement hook: events around the launches of the hot kernels, each record
+    // with its kernel class and algorithmic bytes
     bool prof = false;
     struct ProfRec {
         cudaEvent_t a, b;
         double bytes;
+        const char* name;
     };
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> prof_pool;
@@ -175,6 +177,31 @@ struct esl_net {
 };
 
 namespace esl {
+
+// Measurement hook: when profiling is on, CUDA events on the context's stream bracket
+// the launches made while the scope lives; the record carries the kernel class and
+// the algorithmic bytes of those launches.
+struct ProfScope {
+    esl_ctx* ctx;
+    cudaEvent_t a = nullptr;
+    const char* name;
+    double bytes;
+    ProfScope(esl_ctx* c, const char* nm, double b) : ctx(c && c->prof ? c : nullptr), name(nm), bytes(b) {
+        if (ctx) {
+            a = ctx->prof_event();
+            cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~ProfScope() {
+        if (ctx) {
+            cudaEvent_t e = ctx->prof_event();
+            cudaEventRecord(e, ctx->stream);
+            ctx->prof_recs.push_back({a, e, bytes, name});
+        }
+    }
+    ProfScope(const ProfScope&) = delete;
+    ProfScope& operator=(const ProfScope&) = delete;
+};
 
 // table.cu
 struct DevModel {

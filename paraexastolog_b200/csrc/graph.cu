@@ -278,6 +278,10 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     };
     // budgets: a sweep can only fail to progress once per state
     const int64_t budget = (int64_t)N + 64;
+    // nominal algorithmic bytes of one fixpoint sweep (measurement hook): one pass over
+    // every state's mask, label and colour / level word, 4 B each.  States already
+    // assigned read only their label, so later sweeps move less than this.
+    const double sweep_bytes = 12.0 * (double)N;
 
     ESL_TRY(net->labels.alloc(N));
     int32_t* lab = net->labels.get();
@@ -292,6 +296,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
 
     auto trim = [&]() -> int {
         return fixpoint(fl, [&]() -> int {
+            ProfScope ps(ctx, "graph_sweep", sweep_bytes);
             ESL_COUNT_LAUNCH();
             k_trim<<<nb, kThreads, 0, s>>>(n, N, F, G, lab, ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
@@ -308,6 +313,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         k_color_init<<<nb, kThreads, 0, s>>>(N, lab, color.get(), reached.get());
         ESL_CUDA(cudaGetLastError());
         ESL_TRY(fixpoint(fl, [&]() -> int {
+            ProfScope ps(ctx, "graph_sweep", sweep_bytes);
             ESL_COUNT_LAUNCH();
             k_color_fw<<<nb, kThreads, 0, s>>>(N, G, lab, color.get(), ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
@@ -317,6 +323,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
         k_root_init<<<nb, kThreads, 0, s>>>(N, lab, color.get(), reached.get());
         ESL_CUDA(cudaGetLastError());
         ESL_TRY(fixpoint(fl, [&]() -> int {
+            ProfScope ps(ctx, "graph_sweep", sweep_bytes);
             ESL_COUNT_LAUNCH();
             k_reach_bw<<<nb, kThreads, 0, s>>>(N, F, lab, color.get(), reached.get(), ctx->d_flag.get());
             ESL_CUDA(cudaGetLastError());
@@ -346,6 +353,7 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     k_fill<<<nb, kThreads, 0, s>>>(N, level.get(), 0);
     ESL_CUDA(cudaGetLastError());
     ESL_TRY(fixpoint(fl, [&]() -> int {
+        ProfScope ps(ctx, "graph_sweep", sweep_bytes);
         ESL_COUNT_LAUNCH();
         k_level<<<nb, kThreads, 0, s>>>(N, F, lab, level.get(), ctx->d_flag.get());
         ESL_CUDA(cudaGetLastError());

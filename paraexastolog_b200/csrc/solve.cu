@@ -906,7 +906,7 @@ int inner_bicgstab(esl_ctx* ctx, Layout L, const double* rates, int K, const dou
             k_apply<FWD, 0, T, T><<<g1, kT, 0, s>>>(L, rates, iv.ph, iv.w, dS, nullptr, iv.r0, iv.v, st);
             if (ctx->prof) {
                 cudaEventRecord(eb, s);
-                ctx->prof_recs.push_back({ea, eb, schur_bytes(L, active, sizeof(T))});
+                ctx->prof_recs.push_back({ea, eb, schur_bytes(L, active, sizeof(T)), "schur_operator_whole_system"});
             }
             ESL_COUNT_LAUNCH();
             k_scal_alpha<<<sb, 128, 0, s>>>(K, st);

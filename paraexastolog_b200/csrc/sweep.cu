@@ -1575,53 +1575,60 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 TT* D = (TT*)vD;
                 TT* WW = (TT*)(sizeof(TT) == 8 ? (void*)W64 : WT);
                 const TT* dS = (const TT*)(sizeof(TT) == 8 ? (void*)dS64 : (void*)dS32);
-                // measurement hook: one operator application (k_sw_elim + k_sw_apply) per
-                // iteration of the first poll window, when every started system still runs
-                const int nrun = h_cnt[0];
-                const double op_bytes = (double)nrun * sizeof(TT) * (4.0 * g.no + 2.0 * g.ne) +
-                                        12.0 * (g.ne + g.no) + 4.0 * (double)g.nin;
+                // measurement hook: the launches of the first poll window, when every
+                // started system still runs.  Algorithmic bytes per running system: the
+                // operator moves every vector it touches once (the gathered vector too),
+                // leaving out the per-row out-rate streams that a kernel could recompute;
+                // the row structure (12 B per row, 4 B per predecessor entry) is shared.
+                const double nrun = h_cnt[0];
+                const double row_bytes = 12.0 * (g.ne + g.no) + 4.0 * (double)g.nin;
+                const double op2_bytes = nrun * sizeof(TT) * (2.0 * g.ne + 4.0 * g.no) + row_bytes;
+                const double op6_bytes = nrun * sizeof(TT) * (2.0 * g.ne + 5.0 * g.no) + row_bytes;
+                const double s_bytes = nrun * sizeof(TT) * 4.0 * g.no, xrp_bytes = nrun * sizeof(TT) * 10.0 * g.no;
                 ESL_COUNT_LAUNCH();
                 k_sw_start<TT><<<goi, kSwT, 0, s>>>(a, sc.c[C_SCALE], R64, dS, R, R0, D, PH, V);
                 // kSwPoll iterations; `par` picks the running-count slot of this poll window
                 auto launch_chunk = [&](int par, bool record) -> int {
+                    esl_ctx* pc = record ? ctx : nullptr;
                     for (int j = 0; j < kSwPoll; j++) {
-                    const bool rec = record;
-                    cudaEvent_t ea = nullptr, eb = nullptr;
-                    if (rec) {
-                        ea = ctx->prof_event();
-                        eb = ctx->prof_event();
-                        ESL_CUDA(cudaEventRecord(ea, s));
+                    {
+                        ProfScope ps(pc, "schur_operator", op2_bytes);
+                        ESL_COUNT_LAUNCH();
+                        if (s2)
+                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                        else
+                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
+                        ESL_COUNT_LAUNCH();
+                        if (s2)
+                            k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
+                        else
+                            k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
                     }
-                    ESL_COUNT_LAUNCH();
-                    if (s2)
-                        k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, PH, WW);
-                    else
-                        k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, PH, WW);
-                    ESL_COUNT_LAUNCH();
-                    if (s2)
-                        k_sw_apply<2, 2, TT><<<goi2, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
-                    else
-                        k_sw_apply<1, 2, TT><<<goi, kSwT, smT, s>>>(a, PH, WW, nullptr, R0, V, sc.c[C_R0V], nullptr, nullptr, nullptr);
-                    if (rec) {
-                        ESL_CUDA(cudaEventRecord(eb, s));
-                        ctx->prof_recs.push_back({ea, eb, op_bytes});
+                    {
+                        ProfScope ps(pc, "bicgstab_update", s_bytes);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
                     }
-                    ESL_COUNT_LAUNCH();
-                    k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
-                    ESL_COUNT_LAUNCH();
-                    if (s2)
-                        k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, SH, WW);
-                    else
-                        k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
-                    ESL_COUNT_LAUNCH();
-                    if (s2)
-                        k_sw_apply<2, 6, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                      sc.c[C_TT], R0, sc.c[C_R0T]);
-                    else
-                        k_sw_apply<1, 6, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
-                                                                      sc.c[C_TT], R0, sc.c[C_R0T]);
-                    ESL_COUNT_LAUNCH();
-                    k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                    {
+                        ProfScope ps(pc, "schur_operator", op6_bytes);
+                        ESL_COUNT_LAUNCH();
+                        if (s2)
+                            k_sw_elim<2, TT, TT, TT><<<gei2, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                        else
+                            k_sw_elim<1, TT, TT, TT><<<gei, kSwT, smT, s>>>(a, nullptr, SH, WW);
+                        ESL_COUNT_LAUNCH();
+                        if (s2)
+                            k_sw_apply<2, 6, TT><<<goi2, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                          sc.c[C_TT], R0, sc.c[C_R0T]);
+                        else
+                            k_sw_apply<1, 6, TT><<<goi, kSwT, smT, s>>>(a, SH, WW, nullptr, dS, Tt, sc.c[C_TS],
+                                                                          sc.c[C_TT], R0, sc.c[C_R0T]);
+                    }
+                    {
+                        ProfScope ps(pc, "bicgstab_update", xrp_bytes);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                    }
                     ESL_COUNT_LAUNCH();
                     k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
                                                  d_cnt + 1 + par);

@@ -32,6 +32,9 @@ constexpr size_t kStaticStates = (size_t)1 << kStaticMaxNodes;
 constexpr size_t kStaticBlocks = kStaticStates / 4096;  // flip-mask blocks cover 4096 states each
 constexpr size_t kStaticClauses = ESL_STATIC_TABLE_MAX_CLAUSES;
 constexpr size_t kScanTempBytes = 64 * 1024;
+// The CSC offsets are int32: at most n * 2^n edges must fit below 2^31.
+static_assert(((int64_t)kStaticMaxNodes << kStaticMaxNodes) < (int64_t)INT32_MAX,
+              "ESL_STATIC_TABLE_MAX_NODES allows more edges than int32 CSC offsets hold");
 
 // byte offsets of the regions inside the scratch array (each 256-byte aligned)
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -48,7 +51,9 @@ __device__ __align__(256) unsigned char g_table_scratch[kScratchBytes];
 
 // Device address of g_table_scratch per device.  In host code the symbol is a
 // host-side stand-in, never a device address, so it is looked up once per device
-// with that device current.
+// with that device current.  The cached address belongs to the device's primary
+// context: after cudaDeviceReset it is stale, and the process must not call this
+// entry point on that device again.
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
 unsigned char* g_scratch_addr[kMaxDevices] = {};

@@ -251,7 +251,9 @@ def python_reference(ref: str, models: dict, max_nodes: int = 12):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/paraExaStoLog")
+    ref = sys.argv[1]
     data = os.path.join(ref, "data")
     names = ["toy.bnet", "toy2.bnet", "toy3.bnet", "krasmodel15vars.bnet", "mammalian_cc.bnet",
              "EMT_cohen_ModNet.bnet", "zanudo_expanded.bnet"]
