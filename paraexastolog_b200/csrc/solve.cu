@@ -528,24 +528,38 @@ __global__ void k_terminal_mass(int n, int T, int term_states, int nrhs, size_t 
                                 const double* __restrict__ zE, const double* __restrict__ zO,
                                 double* __restrict__ y) {
     const int k = blockIdx.y;
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= term_states) return;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int b = k / nrhs, r = k % nrhs;
     const double* rt = rates + (size_t)b * 2 * n;
-    uint32_t v = (uint32_t)order[p];
-    int t = term_of[v];
-    double acc = x0[(size_t)r * x0_ld + v];
-    uint32_t g = G[v];
-    while (g) {
-        int i = __ffs(g) - 1;
-        g &= g - 1;
-        uint32_t u = v ^ (1u << i);
-        if (term_of[u] >= 0) continue;
-        uint32_t hu = u >> 1;
-        double zu = (__popc(u) & 1) ? zO[(size_t)k * ld + hu] : zE[(size_t)k * ld + hu];
-        acc += rt[2 * i + ((u >> i) & 1u)] * zu;
+    int t = -1;
+    double acc = 0.0;
+    if (p < term_states) {
+        const uint32_t v = (uint32_t)order[p];
+        t = term_of[v];
+        acc = x0[(size_t)r * x0_ld + v];
+        uint32_t g = G[v];
+        while (g) {
+            int i = __ffs(g) - 1;
+            g &= g - 1;
+            uint32_t u = v ^ (1u << i);
+            if (term_of[u] >= 0) continue;
+            uint32_t hu = u >> 1;
+            double zu = (__popc(u) & 1) ? zO[(size_t)k * ld + hu] : zE[(size_t)k * ld + hu];
+            acc += rt[2 * i + ((u >> i) & 1u)] * zu;
+        }
     }
-    atomicAdd(&y[(size_t)k * T + t], acc);
+    // Positions are grouped by terminal SCC, so the lanes of one SCC are a contiguous
+    // run of the warp: a segmented suffix sum leaves the run's total in its first lane,
+    // which adds it with one atomic (fewer, larger additions round less).
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double va = __shfl_down_sync(0xFFFFFFFFu, acc, o);
+        const int ta = __shfl_down_sync(0xFFFFFFFFu, t, o);
+        if (lane + o < 32 && ta == t) acc += va;
+    }
+    const int tprev = __shfl_up_sync(0xFFFFFFFFu, t, 1);
+    if (t >= 0 && (lane == 0 || tprev != t)) atomicAdd(&y[(size_t)k * T + t], acc);
 }
 
 // x_inf[k][v] = R_b[pos] * y[k][t] on terminal states; marginals accumulated
@@ -569,7 +583,7 @@ __global__ void k_scatter_xinf(int n, int T, int term_states, int nrhs, size_t N
 // ---- dense terminal kernels ----------------------------------------------------------
 // One CTA per (terminal SCC of size 2..kDenseTerm, rate set).  A = K_C with the last row
 // replaced by ones; solve A pi = e_last by Gaussian elimination with partial pivoting.
-constexpr int kDenseTerm = 128;
+constexpr int kDenseTerm = kDenseTerminalMax;
 
 __global__ void __launch_bounds__(256) k_dense_terminal(int n, const int32_t* __restrict__ sccs,
                                                         const int32_t* __restrict__ offsets,
@@ -1661,8 +1675,24 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_CUDA(cudaGetLastError());
             ESL_CUDA(cudaStreamSynchronize(s));  // d_list is reused below
         }
-        if (!big_list.empty()) {
-            // pin one high-mass state per (big terminal SCC, rate set); solve the rest with Krylov
+        if (!big_list.empty() && sweep_supported(net)) {
+            // deflated FP64 Krylov on the odd-row Schur complement of each big terminal SCC
+            SweepStats sw;
+            const int rc = sweep_terminal(ctx, net, B, d_rates, o, Rb, sw);
+            agg.iters += sw.iters;
+            agg.relres = std::max(agg.relres, sw.relres);
+            if (rc != ESL_OK) {
+                if (rep) {
+                    rep->iterations = agg.iters;
+                    rep->refinements = agg.refinements;
+                    rep->relres = agg.relres;
+                    rep->converged = 0;
+                }
+                return rc;
+            }
+        } else if (!big_list.empty()) {
+            // networks beyond the level sweep's 26 nodes: pin one high-mass state per
+            // (big terminal SCC, rate set) and solve the rest with Krylov
             std::vector<uint8_t> h_big(T, 0);
             for (int t : big_list) h_big[t] = 1;
             uint8_t* d_big = (uint8_t*)ws.get(S_BIG, T, &st_);
@@ -1730,7 +1760,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         SweepStats sw;
         int rc = sweep_forward(ctx, net, K, R, d_rates, d_x0, N, o, y, sw);
         agg.iters += sw.iters;
-        agg.relres = sw.relres;
+        agg.relres = std::max(agg.relres, sw.relres);
         if (rc == ESL_ERR_NOT_CONVERGED && !sw.failed.empty()) {
             const int Kf = (int)sw.failed.size();
             if (debug_enabled()) fprintf(stderr, "[esl] sweep: block-solve fallback for %d of %d systems\n", Kf, K);

@@ -61,8 +61,11 @@ constexpr int SW_RUN = 4;    // runs an inner solve in this refinement step
 constexpr int SW_IDONE = 8;  // its inner solve has stopped
 
 // per-system scalar arrays (doubles), each Kp long
+// C_GAM0..2: the deflation scalar gamma(x) of the operator applications of the true
+// residual, of v = A p and of t = A s (deflated groups only); C_D0..2 take the
+// accumulations of the undeflated products there, which nothing reads.
 enum Scal { C_BB, C_RR64, C_PREV, C_RHO, C_R0V, C_TS, C_TT, C_RR, C_RN, C_BETA, C_OMEGA, C_TARGET, C_BEST, C_SCALE,
-            C_R0T, C_NSCAL };
+            C_R0T, C_GAM0, C_GAM1, C_GAM2, C_D0, C_D1, C_D2, C_NSCAL };
 // per-system int arrays
 enum IScal { I_FLAGS, I_ITERS, I_NOIMP, I_TOTAL, I_STALL, I_NISCAL };
 
@@ -73,6 +76,8 @@ struct SwGroup {
     uint32_t scc0, nscc;   // local groups: range in the local SCC list (SCCs of >= 2 states)
     int max_odd;           // local groups: most odd rows of one SCC
     uint64_t nin;          // in-group predecessor entries of the group's rows
+    int term;              // terminal plan: the terminal SCC of the group (-1 otherwise)
+    uint32_t pos0;         // terminal plan: position of the SCC's first state in the order
 };
 
 struct SweepPlan {
@@ -87,6 +92,15 @@ struct SweepPlan {
     DevBuf<uint32_t> lsc_off;            // local SCCs: offsets into lsc_slots
     DevBuf<uint32_t> lsc_ne;             // local SCCs: number of even-parity slots (listed first)
     DevBuf<uint32_t> lsc_slots;          // local SCCs: slots, SCC by SCC
+    // terminal plan: per slot, the state's position in the reordering
+    DevBuf<uint32_t> pos;
+    // the terminal SCCs above kDenseTerminalMax states, one deflated grid group each
+    // (slots of their own; in-group predecessor lists only), or null
+    SweepPlan* term = nullptr;
+    SweepPlan() = default;
+    SweepPlan(const SweepPlan&) = delete;
+    SweepPlan& operator=(const SweepPlan&) = delete;
+    ~SweepPlan() { delete term; }
 };
 
 void free_plan_sweep(void* p) { delete static_cast<SweepPlan*>(p); }
@@ -104,6 +118,10 @@ struct SwArgs {
     // the out-masks): q of the odd rows and 1 / q of the even rows
     const double* Qo;
     const double* IQe;
+    // Deflated groups (a terminal SCC): per-system accumulator of gamma(x) = sum of the
+    // odd-row vector plus sum of its even-row elimination, or null; u_o = q_o * inv_s.
+    double* gam;
+    double inv_s;
 };
 
 // A tile is KT systems of one row handled by TR = KT / S threads, S systems per thread:
@@ -321,7 +339,9 @@ __global__ void __launch_bounds__(kSwT) k_sw_qrows(SwArgs a, double* __restrict_
 // Even-row elimination: W_e = (C_e + sum over in-group odd predecessors o of
 // rate(o -> e) X_o) / q_e.  C (FP64, even rows of the group buffer) and X may be null.
 // S systems per thread.
-template <int S, class TX, class TW, class TC>
+// DEFL: also adds the sum of the written W over the even rows into a.gam (FP64, the
+// deflated operator of a terminal SCC).
+template <int S, class TX, class TW, class TC, bool DEFL = false>
 __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __restrict__ C, const TX* __restrict__ X,
                                                   TW* __restrict__ W) {
     extern __shared__ unsigned char s_raw[];
@@ -330,14 +350,18 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
     sw_rates(s_rate, a, t);
     bool act[S];
     bool any = false;
+    double wsum[S];
 #pragma unroll
     for (int q = 0; q < S; q++) {
         act[q] = !sw_skip(a, t.k + q * t.TR);
         any |= act[q];
+        wsum[q] = 0.0;
     }
-    if (!__any_sync(0xffffffffu, any)) return;
+    // the gathers shuffle across the warp: a warp runs the row loop if any lane is active
+    const bool wany = __any_sync(0xffffffffu, any);
+    if (!DEFL && !wany) return;
     const uint32_t obase = a.beg + a.ne;
-    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne; r += gridDim.x * t.RB) {
+    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < (wany ? a.ne : 0u); r += gridDim.x * t.RB) {
         // (state, out-mask, first entry, count) in one load
         const uint4 d = a.desc[a.beg + r];
         const size_t idx = (size_t)r * a.Kp + t.k;
@@ -348,14 +372,29 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
         if (sizeof(TC) == 8 && a.IQe) {
 #pragma unroll
             for (int q = 0; q < S; q++)
-                if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] * (TC)__ldcs(a.IQe + idx + q * t.TR));
+                if (act[q]) {
+                    const TW w = (TW)(acc[q] * (TC)__ldcs(a.IQe + idx + q * t.TR));
+                    W[idx + q * t.TR] = w;
+                    if (DEFL) wsum[q] += (double)w;
+                }
         } else {
             TC qv[S];
             sw_qs<S>(s_rate, d.x, d.y, t, qv);
 #pragma unroll
             for (int q = 0; q < S; q++)
-                if (act[q]) W[idx + q * t.TR] = (TW)(acc[q] / qv[q]);
+                if (act[q]) {
+                    const TW w = (TW)(acc[q] / qv[q]);
+                    W[idx + q * t.TR] = w;
+                    if (DEFL) wsum[q] += (double)w;
+                }
         }
+    }
+    if (DEFL) {
+        double v[1][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) v[0][q] = wsum[q];
+        double* const dst[1] = {a.gam};
+        sw_reduce<1, S>(v, dst, t, a.K);
     }
 }
 
@@ -369,7 +408,9 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
 //           x / r update: beta = -(r0 . t) / (r0 . v))
 // S systems per thread.  X, AUX and Y are streamed (evict-first) so that the gathered W
 // keeps its place in L2.
-template <int S, int MODE, class T>
+// DEFL (MODE 1, 2 and 6): also adds the sum of X over the odd rows into a.gam; Y is
+// then the undeflated product, which k_sw_defl_fin completes.
+template <int S, int MODE, class T, bool DEFL = false>
 __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict__ X, const T* __restrict__ W,
                                                    const double* __restrict__ B, const T* __restrict__ AUX,
                                                    T* __restrict__ Y, double* acc0, double* acc1,
@@ -378,12 +419,12 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
     T* s_rate = reinterpret_cast<T*>(s_raw);
     const Tile t = tile_of<S>(a.KT);
     sw_rates(s_rate, a, t);
-    double d0[S], d1[S], d2[S];
+    double d0[S], d1[S], d2[S], dg[S];
     bool act[S];
     bool any = false;
 #pragma unroll
     for (int q = 0; q < S; q++) {
-        d0[q] = d1[q] = d2[q] = 0.0;
+        d0[q] = d1[q] = d2[q] = dg[q] = 0.0;
         const int k = t.k + q * t.TR;
         act[q] = !((MODE >= 2) ? sw_skip(a, k) : (k >= a.K));
         any |= act[q];
@@ -415,6 +456,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
                     d0[q] += y * y;
                 } else {
                     const T x = __ldcs(X + i);
+                    if (DEFL) dg[q] += (double)x;
                     const T y = qv[q] * x - flow[q];
                     if (MODE == 1) {
                         const double res = B[i] - (double)y;
@@ -436,7 +478,27 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
             }
         }
     }
-    if (MODE == 6) {
+    if (DEFL && MODE == 6) {
+        double v[4][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) {
+            v[0][q] = d0[q];
+            v[1][q] = d1[q];
+            v[2][q] = d2[q];
+            v[3][q] = dg[q];
+        }
+        double* const dst[4] = {acc0, acc1, acc2, a.gam};
+        sw_reduce<4, S>(v, dst, t, a.K);
+    } else if (DEFL) {
+        double v[2][S];
+#pragma unroll
+        for (int q = 0; q < S; q++) {
+            v[0][q] = d0[q];
+            v[1][q] = dg[q];
+        }
+        double* const dst[2] = {acc0, a.gam};
+        sw_reduce<2, S>(v, dst, t, a.K);
+    } else if (MODE == 6) {
         double v[3][S];
 #pragma unroll
         for (int q = 0; q < S; q++) {
@@ -462,6 +524,100 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
         double* const dst[1] = {acc0};
         sw_reduce<1, S>(v, dst, t, a.K);
     }
+}
+
+// ---- deflated operator of a terminal SCC -------------------------------------------------
+// For a terminal SCC C the stationary vector solves (-K_C + u 1^T) pi = u, whose only
+// solution is the normalised kernel of K_C whenever 1^T u != 0 (1^T K_C = 0), and whose
+// matrix keeps every eigenvalue of -K_C except 0, which moves to 1^T u.  With u zero on
+// the even rows the even rows still eliminate exactly, and on the odd rows the system
+// becomes S x + u gamma(x) = u with gamma(x) = 1^T x + 1^T W(x), W the even-row
+// elimination.  Here u_o = q_o / s (s = states of the SCC), so 1^T u is about the mean
+// out-rate.  k_sw_elim / k_sw_apply<DEFL> accumulate gamma; this kernel adds gamma u to
+// the product (MODE 2, 6) or subtracts it from the residual (MODE 1) and forms the
+// products of that MODE (see k_sw_apply) on the completed vector.
+template <int MODE>
+__global__ void __launch_bounds__(kSwT) k_sw_defl_fin(SwArgs a, double* __restrict__ Y, const double* __restrict__ X,
+                                                      const double* __restrict__ AUX, const double* __restrict__ R0x,
+                                                      const double* __restrict__ gam, double* acc0, double* acc1,
+                                                      double* acc2) {
+    const Tile t = tile_of(a.KT);
+    const bool act = MODE == 1 ? t.k < a.K : !sw_skip(a, t.k);
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    if (act) {
+        const double g = gam[t.k];
+        for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
+            const size_t i = (size_t)r * a.Kp + t.k;
+            const double u = a.Qo[i] * a.inv_s;
+            if (MODE == 1) {
+                const double y = Y[i] - g * u;
+                Y[i] = y;
+                d0 += y * y;
+            } else {
+                const double y = Y[i] + g * u;
+                Y[i] = y;
+                if (MODE == 2) {
+                    d0 += AUX[i] * y;
+                } else {
+                    d0 += y * (AUX[i] * X[i]);
+                    d1 += y * y;
+                    d2 += R0x[i] * y;
+                }
+            }
+        }
+    }
+    if (MODE == 6) {
+        double v[3][1] = {{d0}, {d1}, {d2}};
+        double* const dst[3] = {acc0, acc1, acc2};
+        sw_reduce<3>(v, dst, t, a.K);
+    } else {
+        double v[1][1] = {{d0}};
+        double* const dst[1] = {acc0};
+        sw_reduce<1>(v, dst, t, a.K);
+    }
+}
+
+// Right-hand side of a deflated group in the group buffer: 0 on the even rows, u_o =
+// q_o / s on the odd rows.
+__global__ void __launch_bounds__(kSwT) k_sw_defl_rhs(SwArgs a, double* __restrict__ Bv) {
+    extern __shared__ double s_rate[];
+    const Tile t = tile_of(a.KT);
+    sw_rates(s_rate, a, t);
+    if (t.k >= a.K) return;
+    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne + a.no; r += gridDim.x * t.RB) {
+        const uint2 row = a.rows[a.beg + r];
+        Bv[(size_t)r * a.Kp + t.k] = r < a.ne ? 0.0 : sw_q(s_rate, row.x, row.y, t) * a.inv_s;
+    }
+}
+
+// Terminal kernel of a deflated group into Rb[k][position]: the group's slots (both
+// parities, solved in Z) at their positions in the reordering, and their sum per system.
+__global__ void __launch_bounds__(kSwT) k_sw_term_out(SwArgs a, const uint32_t* __restrict__ pos,
+                                                      const double* __restrict__ Z, int TS, double* __restrict__ Rb,
+                                                      double* sums) {
+    const Tile t = tile_of(a.KT);
+    double d = 0.0;
+    if (t.k < a.K) {
+        for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.ne + a.no; r += gridDim.x * t.RB) {
+            const uint32_t slot = a.beg + r;
+            const double v = Z[(size_t)slot * a.Kp + t.k];
+            Rb[(size_t)t.k * TS + pos[slot]] = v;
+            d += v;
+        }
+    }
+    double v[1][1] = {{d}};
+    double* const dst[1] = {sums};
+    sw_reduce<1>(v, dst, t, a.K);
+}
+
+// Rb[k][p0 .. p0 + count) /= sums[k]
+__global__ void k_sw_term_norm(int K, int TS, uint32_t p0, uint32_t count, const double* __restrict__ sums,
+                               double* __restrict__ Rb) {
+    const int k = blockIdx.y;
+    if (k >= K) return;
+    const double inv = sums[k] != 0.0 ? 1.0 / sums[k] : 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        Rb[(size_t)k * TS + p0 + i] *= inv;
 }
 
 // ---- BiCGStab vector steps (odd rows; scalars per system) --------------------------------
@@ -547,6 +703,7 @@ __global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int stall_max, int
             cnt++;
         }
         sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = sc.c[C_R0T][k] = 0.0;
+        sc.c[C_GAM1][k] = sc.c[C_GAM2][k] = 0.0;
     }
     atomicAdd(&s_cnt, cnt);
     __syncthreads();
@@ -586,6 +743,7 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
         sc.c[C_BEST][k] = 1.0;
         sc.i[I_STALL][k] = 0;
         sc.c[C_R0V][k] = sc.c[C_TS][k] = sc.c[C_TT][k] = sc.c[C_RR][k] = sc.c[C_RN][k] = sc.c[C_R0T][k] = 0.0;
+        sc.c[C_GAM1][k] = sc.c[C_GAM2][k] = 0.0;
         cnt++;
     }
     atomicAdd(&s_cnt, cnt);
@@ -1022,6 +1180,85 @@ enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R,
 
 bool debug_on();
 
+// Terminal plan: one grid group per terminal SCC above kDenseTerminalMax states, its
+// even-parity states first; predecessor entries only from the same SCC (a terminal SCC
+// receives edges from transient states too, which its kernel does not see).
+int build_terminal_plan(const std::vector<int32_t>& order, const std::vector<int32_t>& offsets, int T,
+                        const std::vector<uint32_t>& F, const std::vector<uint32_t>& G, cudaStream_t s,
+                        SweepPlan*& out) {
+    out = nullptr;
+    bool any = false;
+    for (int t = 0; t < T; t++) any |= offsets[t + 1] - offsets[t] > kDenseTerminalMax;
+    if (!any) return ESL_OK;
+    auto* TP = new SweepPlan();
+    std::vector<uint32_t> tslot(F.size(), 0xFFFFFFFFu);
+    std::vector<uint2> rows;
+    std::vector<uint32_t> pos;
+    for (int t = 0; t < T; t++) {
+        const int sz = offsets[t + 1] - offsets[t];
+        if (sz <= kDenseTerminalMax) continue;
+        SwGroup g{};
+        g.beg = (uint32_t)rows.size();
+        g.kind = 2;
+        g.max_scc = sz;
+        g.term = t;
+        g.pos0 = (uint32_t)offsets[t];
+        for (int par = 0; par < 2; par++) {
+            for (int p = offsets[t]; p < offsets[t + 1]; p++) {
+                const uint32_t v = (uint32_t)order[p];
+                if ((uint32_t)(__builtin_popcount(v) & 1) != (uint32_t)par) continue;
+                tslot[v] = (uint32_t)rows.size();
+                rows.push_back(make_uint2(v, F[v]));
+                pos.push_back((uint32_t)p);
+            }
+            (par ? g.no : g.ne) = (uint32_t)rows.size() - g.beg - (par ? g.ne : 0);
+        }
+        TP->max_rows = std::max(TP->max_rows, g.ne + g.no);
+        TP->max_even = std::max(TP->max_even, g.ne);
+        TP->max_odd = std::max(TP->max_odd, g.no);
+        TP->groups.push_back(g);
+    }
+    const uint32_t M = (uint32_t)rows.size();
+    TP->M = M;
+    std::vector<uint32_t> ig_ptr(M + 1, 0), ig;
+    for (uint32_t sl = 0; sl < M; sl++) {
+        const uint32_t v = rows[sl].x;
+        uint32_t in = G[v];
+        while (in) {
+            const int i = __builtin_ctz(in);
+            in &= in - 1;
+            const uint32_t su = tslot[v ^ (1u << i)];
+            if (su == 0xFFFFFFFFu) continue;  // a transient predecessor
+            ig.push_back((su << 6) | (2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u)));
+        }
+        ig_ptr[sl + 1] = (uint32_t)ig.size();
+    }
+    for (SwGroup& g : TP->groups) g.nin = ig_ptr[g.beg + g.ne + g.no] - ig_ptr[g.beg];
+    std::vector<uint4> desc(M);
+    for (uint32_t sl = 0; sl < M; sl++)
+        desc[sl] = make_uint4(rows[sl].x, rows[sl].y, ig_ptr[sl], ig_ptr[sl + 1] - ig_ptr[sl]);
+    int rc = ESL_OK;
+    auto up = [&](auto& d, const auto& h) {
+        if (rc != ESL_OK) return;
+        rc = d.alloc(std::max<size_t>(h.size(), 1));
+        if (rc == ESL_OK && !h.empty() &&
+            cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(h[0]), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            rc = fail(ESL_ERR_CUDA, "terminal plan upload failed");
+    };
+    up(TP->rows, rows);
+    up(TP->desc, desc);
+    up(TP->ig_ptr, ig_ptr);
+    up(TP->ig_ent, ig);
+    up(TP->pos, pos);
+    if (rc == ESL_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(ESL_ERR_CUDA, "terminal plan upload failed");
+    if (rc != ESL_OK) {
+        delete TP;
+        return rc;
+    }
+    out = TP;
+    return ESL_OK;
+}
+
 int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     // one builder at a time, so that threads solving the same network share one plan
     static std::mutex mu;
@@ -1062,6 +1299,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
         SwGroup g{};
         g.beg = (uint32_t)rows.size();
         g.max_scc = mx;
+        g.term = -1;
         g.kind = mx == 1 ? 0 : (mx <= kSwLocalMax ? 1 : 2);
         for (int par = 0; par < 2; par++) {
             for (int p = offsets[c]; p < offsets[c1]; p++) {
@@ -1206,6 +1444,7 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     up32(P->lsc_ne, lsc_ne);
     up32(P->lsc_slots, lsc_slots);
     if (rc == ESL_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(ESL_ERR_CUDA, "sweep plan upload failed");
+    if (rc == ESL_OK) rc = build_terminal_plan(order, offsets, T, F, G, s, P->term);
     if (rc != ESL_OK) {
         delete P;
         return rc;
@@ -1318,17 +1557,21 @@ int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& state
 // slots are packed into 26 bits of a predecessor entry
 bool sweep_supported(const esl_net* net) { return net->n >= 1 && net->n <= 26; }
 
-int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
-                  size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st) {
-    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
-    SweepPlan* P = nullptr;
-    ESL_TRY(build_plan(ctx, net, P));
+namespace {
+
+// The group loop of the level sweep over plan P.  Transient mode (term == false): the
+// groups of the transient states, y[k * T + t] += mass into terminal SCC t.  Terminal
+// mode: the deflated groups of the big terminal SCCs (P = the terminal plan, nrhs = 1,
+// x0 unused), their normalised kernels into y = Rb[k][position], FP64 throughout.
+int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, int nrhs, const double* rates,
+              const double* x0, size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st) {
     if (!ctx->sweep_work) ctx->sweep_work = new Workspace();
     Workspace& ws = *static_cast<Workspace*>(ctx->sweep_work);
     cudaStream_t s = ctx->stream;
     const int n = net->n, T = net->T;
     const int Kp = (K + 31) & ~31;
-    const bool mixed = o.method == ESL_METHOD_MIXED;
+    const bool mixed = !term && o.method == ESL_METHOD_MIXED;
+    const bool defl = term;
     int st_ = ESL_OK;
     double* Z = (double*)ws.get(W_Z, (size_t)std::max<uint32_t>(P->M, 1) * Kp * 8, &st_);
     double* rateT = (double*)ws.get(W_RATET, (size_t)2 * n * Kp * 8, &st_);
@@ -1386,6 +1629,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         a.flags = nullptr;
         a.KT = KT64;
         const uint32_t rows = g.ne + g.no;
+        a.gam = nullptr;
+        a.inv_s = 1.0 / (double)std::max<uint32_t>(rows, 1);
         if (g.kind == 0) {
             ESL_COUNT_LAUNCH();
             k_sw_rhs<true><<<row_grid(rows, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
@@ -1396,8 +1641,11 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         double* Bv = (double*)ws.get(W_BV, (size_t)P->max_rows * Kp * 8, &st_);
         if (st_ != ESL_OK) return st_;
         ESL_COUNT_LAUNCH();
-        k_sw_rhs<false><<<row_grid(rows, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
-            a, P->og_ptr.get(), P->og_ent.get(), x0, x0_ld, Z, Bv);
+        if (term)
+            k_sw_defl_rhs<<<row_grid(rows, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(a, Bv);
+        else
+            k_sw_rhs<false><<<row_grid(rows, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
+                a, P->og_ptr.get(), P->og_ent.get(), x0, x0_ld, Z, Bv);
         ESL_CUDA(cudaGetLastError());
         // ---- Krylov group (CTA-local or grid-wide) ----
         if (g.kind == 1)
@@ -1452,7 +1700,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         k_sw_apply<1, 0, double><<<go, kSwT, gsm64, s>>>(a, nullptr, W64, Bv + (size_t)g.ne * Kp, nullptr, bS,
                                                      sc.c[C_BB], nullptr, nullptr, nullptr);
         ESL_COUNT_LAUNCH();
-        k_sw_init<<<go, kSwT, 0, s>>>(a, o.d_warm, (size_t)net->N, bS, dS64, X64);
+        const double* warm = term ? nullptr : o.d_warm;
+        k_sw_init<<<go, kSwT, 0, s>>>(a, warm, (size_t)net->N, bS, dS64, X64);
         ESL_CUDA(cudaGetLastError());
         if (g.kind == 1) {
             SwLocal l{};
@@ -1524,6 +1773,22 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             a.flags = nullptr;
             a.KT = gKT64;
             ESL_CUDA(cudaMemsetAsync(sc.c[C_RR64], 0, (size_t)Kp * 8, s));
+            if (defl) {
+                // R64 = bS - (S X + gamma(X) u)
+                ESL_CUDA(cudaMemsetAsync(sc.c[C_GAM0], 0, (size_t)Kp * 8, s));
+                SwArgs ad = a;
+                ad.gam = sc.c[C_GAM0];
+                ESL_COUNT_LAUNCH();
+                k_sw_elim<1, double, double, double, true><<<ge, kSwT, gsm64, s>>>(ad, nullptr, X64, W64);
+                ESL_COUNT_LAUNCH();
+                k_sw_apply<1, 1, double, true><<<go, kSwT, gsm64, s>>>(ad, X64, W64, bS, nullptr, R64, sc.c[C_D0],
+                                                                        nullptr, nullptr, nullptr);
+                ESL_COUNT_LAUNCH();
+                k_sw_defl_fin<1><<<go, kSwT, 0, s>>>(ad, R64, nullptr, nullptr, nullptr, sc.c[C_GAM0], sc.c[C_RR64],
+                                                    nullptr, nullptr);
+                ESL_CUDA(cudaGetLastError());
+                return ESL_OK;
+            }
             ESL_COUNT_LAUNCH();
             k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, nullptr, X64, W64);
             ESL_COUNT_LAUNCH();
@@ -1531,7 +1796,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             ESL_CUDA(cudaGetLastError());
             return ESL_OK;
         };
-        if (o.d_warm) {
+        if (warm) {
             // least-squares scale of the warm start per system (C_R0V, C_TS as scratch)
             ESL_CUDA(cudaMemsetAsync(sc.c[C_R0V], 0, (size_t)Kp * 8, s));
             ESL_CUDA(cudaMemsetAsync(sc.c[C_TS], 0, (size_t)Kp * 8, s));
@@ -1561,7 +1826,8 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
             const size_t smT = inner64 ? gsm64 : gsm32;
             const dim3 gei = row_grid(g.ne, Kp, a.KT, ctx->sm_count), goi = row_grid(g.no, Kp, a.KT, ctx->sm_count);
             // two systems per thread in the gather kernels when the tile is wide enough
-            const bool s2 = a.KT >= 64 && (net->tune_s2 >= 0 ? net->tune_s2 != 0 : ctx->tune_s2 != 0);
+            // (not in deflated groups)
+            const bool s2 = !defl && a.KT >= 64 && (net->tune_s2 >= 0 ? net->tune_s2 != 0 : ctx->tune_s2 != 0);
             const dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2),
                        goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
             auto run_inner = [&](auto tag) -> int {
@@ -1591,6 +1857,39 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                 auto launch_chunk = [&](int par, bool record) -> int {
                     esl_ctx* pc = record ? ctx : nullptr;
                     for (int j = 0; j < kSwPoll; j++) {
+                    if (defl) {
+                        // v = A p and t = A s of the deflated operator (FP64 only)
+                        if constexpr (sizeof(TT) == 8) {
+                        SwArgs ad = a;
+                        ad.gam = sc.c[C_GAM1];
+                        ESL_COUNT_LAUNCH();
+                        k_sw_elim<1, TT, TT, TT, true><<<gei, kSwT, smT, s>>>(ad, nullptr, PH, WW);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_apply<1, 2, TT, true><<<goi, kSwT, smT, s>>>(ad, PH, WW, nullptr, R0, V, sc.c[C_D0],
+                                                                         nullptr, nullptr, nullptr);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_defl_fin<2><<<goi, kSwT, 0, s>>>(ad, (double*)V, nullptr, (const double*)R0, nullptr,
+                                                             sc.c[C_GAM1], sc.c[C_R0V], nullptr, nullptr);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                        ad.gam = sc.c[C_GAM2];
+                        ESL_COUNT_LAUNCH();
+                        k_sw_elim<1, TT, TT, TT, true><<<gei, kSwT, smT, s>>>(ad, nullptr, SH, WW);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_apply<1, 6, TT, true><<<goi, kSwT, smT, s>>>(ad, SH, WW, nullptr, dS, Tt, sc.c[C_D0],
+                                                                         sc.c[C_D1], R0, sc.c[C_D2]);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_defl_fin<6><<<goi, kSwT, 0, s>>>(ad, (double*)Tt, (const double*)SH, (const double*)dS,
+                                                             (const double*)R0, sc.c[C_GAM2], sc.c[C_TS],
+                                                             sc.c[C_TT], sc.c[C_R0T]);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                        ESL_COUNT_LAUNCH();
+                        k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
+                                                     d_cnt + 1 + par);
+                        }
+                        continue;
+                    }
                     {
                         ProfScope ps(pc, "schur_operator", op2_bytes);
                         ESL_COUNT_LAUNCH();
@@ -1664,7 +1963,7 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
                             rc = fail(ESL_ERR_CUDA, "graph launch failed");
                         if (rc != ESL_OK) return rc;
                     } else {
-                        count_launches(7 * kSwPoll);
+                        count_launches((defl ? 9 : 7) * kSwPoll);
                         if (cudaGraphLaunch(gexec[par], s) != cudaSuccess)
                             return fail(ESL_ERR_CUDA, "graph launch failed");
                     }
@@ -1700,6 +1999,17 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         ESL_COUNT_LAUNCH();
         k_sw_elim<1, double, double, double><<<ge, kSwT, gsm64, s>>>(a, Bv, X64, Z + (size_t)g.beg * Kp);
         ESL_CUDA(cudaGetLastError());
+        if (term) {
+            // the SCC's kernel at its positions in the reordering, normalised per system
+            double* sums = sc.c[C_D1];
+            ESL_CUDA(cudaMemsetAsync(sums, 0, (size_t)Kp * 8, s));
+            ESL_COUNT_LAUNCH();
+            k_sw_term_out<<<row_grid(rows, Kp, gKT64, ctx->sm_count), kSwT, 0, s>>>(a, P->pos.get(), Z, net->term_states,
+                                                                                   y, sums);
+            ESL_COUNT_LAUNCH();
+            k_sw_term_norm<<<dim3((rows + 255) / 256, K), 256, 0, s>>>(K, net->term_states, g.pos0, rows, sums, y);
+            ESL_CUDA(cudaGetLastError());
+        }
         h_flags.resize(K);
         std::vector<double> h_rr(K), h_bb(K);
         ESL_CUDA(cudaMemcpyAsync(h_flags.data(), sc.i[I_FLAGS], (size_t)K * 4, cudaMemcpyDeviceToHost, s));
@@ -1720,14 +2030,15 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
     // masses into the terminal SCCs
     a.flags = nullptr;
     a.KT = KT64;
-    if (P->TS > 0) {
+    a.gam = nullptr;
+    if (!term && P->TS > 0) {
         ESL_COUNT_LAUNCH();
         k_sw_term<<<row_grid((uint32_t)P->TS, Kp, KT64, ctx->sm_count), kSwT, sm64, s>>>(
             a, P->TS, net->order.get(), net->term_of.get(), P->tp_ptr.get(), P->tp_ent.get(), x0, x0_ld, Z, T, y);
         ESL_CUDA(cudaGetLastError());
     }
     // expected occupation by state (the learned warm start's training label)
-    if (o.d_occupation && P->M > 0) {
+    if (!term && o.d_occupation && P->M > 0) {
         ESL_COUNT_LAUNCH();
         k_sw_occupation<<<dim3((P->M + 31) / 32, Kp / 32), 256, 0, s>>>(P->M, K, Kp, (size_t)net->N, P->rows.get(), Z,
                                                                         o.d_occupation);
@@ -1756,11 +2067,39 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
         if (failed[k]) st.failed.push_back(k);
     if (!st.failed.empty()) {
         char msg[160];
-        snprintf(msg, sizeof msg, "level sweep: %zu of %d systems above the acceptance residual",
-                 st.failed.size(), K);
+        snprintf(msg, sizeof msg, "level sweep%s: %zu of %d systems above the acceptance residual",
+                 term ? " (terminal kernels)" : "", st.failed.size(), K);
         return fail(ESL_ERR_NOT_CONVERGED, msg);
     }
     return ESL_OK;
+}
+
+}  // namespace
+
+int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
+                  size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st) {
+    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
+    SweepPlan* P = nullptr;
+    ESL_TRY(build_plan(ctx, net, P));
+    return sweep_run(ctx, net, P, false, K, nrhs, rates, x0, x0_ld, o, y, st);
+}
+
+int sweep_terminal(esl_ctx* ctx, const esl_net* net, int B, const double* rates, const esl_solve_opts& o, double* Rb,
+                   SweepStats& st) {
+    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
+    SweepPlan* P = nullptr;
+    ESL_TRY(build_plan(ctx, net, P));
+    if (!P->term) return ESL_OK;
+    // terminal kernels can be badly conditioned and cost little next to the transient
+    // part: a tighter tolerance and larger budgets than the transient solve's
+    esl_solve_opts to = o;
+    to.method = ESL_METHOD_DIRECT;
+    to.d_warm = nullptr;
+    to.d_occupation = nullptr;
+    to.tol = std::min(o.tol > 0 ? o.tol : 1e-10, 1e-12);
+    to.max_iters = std::max(o.max_iters, 3000);
+    to.max_refine = std::max(o.max_refine, 8);
+    return sweep_run(ctx, net, P->term, true, B, 1, rates, nullptr, 0, to, Rb, st);
 }
 
 }  // namespace esl

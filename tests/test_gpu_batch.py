@@ -66,3 +66,39 @@ def test_solve_many_reports_a_failing_job(esl):
     jobs[1] = (net, bad, xs)
     with pytest.raises(esl.EslError):
         esl.solve_many(ctxs, jobs, method=esl.METHOD_DIRECT)
+
+
+def test_many_network_workload_full_size(esl):
+    """The many-network workload at its stated size: 48 random networks (n = 12..18,
+    uneven), 64 rate sets x 16 initial distributions each, 49,152 solves in one
+    esl_solve_many call over four contexts.  Every job converges; two seeded (rate set,
+    x0) pairs per network are checked against the FP64 oracle (L1 <= 1e-9)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    w = synth.config_batch()
+    ctxs = [esl.Context(0, torch.cuda.Stream()) for _ in range(4)]
+    jobs = []
+    for i, (net_g, rates, xs) in enumerate(zip(w.networks, w.rates, w.x0)):
+        net = esl.Net.build(ctxs[i % len(ctxs)], esl.Model.parse(net_g.bnet), rates[0])
+        jobs.append((net, rates, xs))
+    res = esl.solve_many(ctxs, jobs, method=esl.METHOD_DIRECT, tol=1e-10)
+    assert sum(r.x_inf.shape[0] * r.x_inf.shape[1] for r in res) == 48 * 64 * 16
+    assert all(r.report.converged == 1 and r.status == 0 for r in res)
+    rng = np.random.default_rng(48)
+    picks = [(rng.integers(0, 64, 2), rng.integers(0, 16, 2)) for _ in range(48)]
+
+    def oracle_job(i):
+        net_g, rates, xs = w.networks[i], w.rates[i], w.x0[i]
+        kb, kq = picks[i]
+        sym = O.Model(text=net_g.bnet).analyse(rates[0])
+        return sym.solve_many(rates[kb], xs[kq], threads=1)
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        refs = list(ex.map(oracle_job, range(48)))
+    for i, (r, (ox, om)) in enumerate(zip(res, refs)):
+        kb, kq = picks[i]
+        got = r.x_inf[torch.as_tensor(kb), torch.as_tensor(kq)].cpu().numpy()
+        gm = r.marginals[torch.as_tensor(kb), torch.as_tensor(kq)].cpu().numpy()
+        assert np.abs(got - ox).sum(1).max() <= 1e-9, i
+        np.testing.assert_allclose(gm, om, atol=1e-9, rtol=0)
