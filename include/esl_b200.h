@@ -117,7 +117,7 @@ int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32
  *      services that allocate only at start-up.  Output is the same CSC as
  *      esl_table_build (d_indptr[N+1], d_rows/d_cols with rows_capacity entries,
  *      d_cols may be NULL), on the given stream of the CURRENT device.  It takes no
- *      context and calls no cudaMalloc/cudaFree: its scratch (~4.2 MB) is a static
+ *      context and calls no cudaMalloc/cudaFree: its scratch (~4.3 MB) is a static
  *      device array that every GPU loading the library keeps until exit.
  *      Limits: at most ESL_STATIC_TABLE_MAX_NODES nodes and
  *      ESL_STATIC_TABLE_MAX_CLAUSES DNF clauses, else ESL_ERR_TOO_LARGE; *nnz

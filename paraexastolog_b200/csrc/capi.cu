@@ -64,10 +64,9 @@ int table_pass(esl_ctx* ctx, const Model& m, const double* rates, DevBuf<uint32_
                DevBuf<uint32_t>& counts, int64_t& nnz, bool want_G) {
     ESL_TRY(check_rates(m, rates));
     cudaStream_t s = ctx->stream;
-    DevBuf<int32_t> off;
-    DevBuf<uint32_t> pos, neg;
+    DevModelBufs mb;
     DevModel dm;
-    ESL_TRY(upload_model(m, off, pos, neg, rates, dm, s));
+    ESL_TRY(upload_model(m, mb, rates, dm, s));
     const uint64_t N = 1ull << m.n();
     ESL_TRY(F.alloc(N));
     if (want_G) ESL_TRY(G.alloc(N));
@@ -433,10 +432,9 @@ int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32
 int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in) {
     if (!ctx || !m || !d_out) return fail(ESL_ERR_INVALID, "NULL argument");
     ESL_TRY(check_rates(m->m, rates));
-    DevBuf<int32_t> off;
-    DevBuf<uint32_t> pos, neg;
+    DevModelBufs mb;
     DevModel dm;
-    ESL_TRY(upload_model(m->m, off, pos, neg, rates, dm, ctx->stream));
+    ESL_TRY(upload_model(m->m, mb, rates, dm, ctx->stream));
     ESL_TRY(launch_flip_masks(dm, d_out, d_in, nullptr, ctx->stream));
     ESL_CUDA(cudaStreamSynchronize(ctx->stream));
     return ESL_OK;

@@ -204,15 +204,42 @@ struct ProfScope {
 };
 
 // table.cu
+// States per count block of the table kernels: k_flip_masks writes one edge count per
+// block, k_emit_csc starts each block's edges at the block's prefix offset.
+constexpr int kTableBlockStates = 1024;
+// Rule tables: node i's rule over the 32 states of a word depends only on the word's
+// bits at the rule's variables of index >= 5 (at most kRuleTableMaxBits of them): a
+// table of 2^k words (and a second one for the rule seen across bit i) replaces the
+// clause loop.  At most kRuleTableMaxWords words in all; other nodes use the clauses.
+constexpr int kRuleTableMaxBits = 8;
+constexpr int kRuleTableMaxWords = 8192;
+constexpr uint32_t kNoRuleTable = 0xFFFFFFFFu;
+struct HostModel {
+    std::vector<int32_t> off;     // clause offsets per node (n + 1)
+    std::vector<uint32_t> pos, neg;
+    std::vector<uint4> info;      // per node: (table offset, table bits or kNoRuleTable, bit positions 0-3, 4-7)
+    std::vector<uint32_t> tab;    // the tables
+    uint32_t self_dep = 0;        // nodes whose rule reads their own bit
+};
+void host_model(const Model& m, HostModel& hm);
 struct DevModel {
     int n;
     const int32_t* off;
     const uint32_t* pos;
     const uint32_t* neg;
+    const uint4* info;
+    const uint32_t* tab;
+    uint32_t tab_words;
     uint32_t up_ok, down_ok, self_dep;
 };
-int upload_model(const Model& m, DevBuf<int32_t>& off, DevBuf<uint32_t>& pos, DevBuf<uint32_t>& neg,
-                 const double* rates, DevModel& dm, cudaStream_t s);
+struct DevModelBufs {
+    DevBuf<int32_t> off;
+    DevBuf<uint32_t> pos, neg, tab;
+    DevBuf<uint4> info;
+};
+int upload_model(const Model& m, DevModelBufs& b, const double* rates, DevModel& dm, cudaStream_t s);
+// zero-rate masks of a rate vector: bit i of up_ok / down_ok = rate 2i / 2i+1 nonzero
+void rate_masks(int n, const double* rates, uint32_t& up_ok, uint32_t& down_ok);
 int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* block_counts, cudaStream_t s);
 int64_t flip_mask_blocks(int n);
 int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
@@ -226,6 +253,10 @@ int build_graph(esl_ctx* ctx, esl_net* net);
 // solve.cu
 void free_workspace(void* w);
 
+// Terminal SCCs of 2..kDenseTerminalMax states get their kernel from a dense FP64 LU
+// (solve.cu); larger ones from the deflated Krylov solve of the level sweep (sweep.cu).
+constexpr int kDenseTerminalMax = 128;
+
 // sweep.cu: state-major level sweep of the transient forward solve.  Adds into
 // y[k * T + t] the mass that terminal SCC t receives in system k (rate set k / nrhs,
 // x0 row k % nrhs).  Systems that miss the tolerance are listed in `failed` (their y
@@ -238,6 +269,12 @@ struct SweepStats {
 bool sweep_supported(const esl_net* net);
 int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const double* rates, const double* x0,
                   size_t x0_ld, const esl_solve_opts& o, double* y, SweepStats& st);
+// Kernels of the terminal SCCs above kDenseTerminalMax states for B rate sets, FP64,
+// into Rb[b][position] (positions of the reordering, B x term_states), normalised to
+// sum 1 per SCC.  Systems that miss the acceptance residual are listed in `failed`
+// (ESL_ERR_NOT_CONVERGED).
+int sweep_terminal(esl_ctx* ctx, const esl_net* net, int B, const double* rates, const esl_solve_opts& o, double* Rb,
+                   SweepStats& st);
 void free_sweep_workspace(void* w);
 // states whose warm start the sweep's grid-wide Krylov groups read (their odd-parity rows)
 int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& states);

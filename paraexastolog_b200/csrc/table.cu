@@ -5,11 +5,12 @@
 // (cuda/src/transition_table.cu:76-119): node i flips up at s when its DNF is true,
 // bit i of s is 0 and rates[2i] != 0; it flips down when the DNF is false, bit i is 1
 // and rates[2i+1] != 0.  The reference evaluates each clause over all 2^n states with
-// one thrust pass per clause, compacts per node and sorts the COO list by column;
-// here one thread evaluates every rule over 32 states at once (one bit per state in a
-// 32-bit word), transposes the n x 32 bit matrix in registers and the edges of a
-// state are emitted already sorted, so no sort is needed.
-#include <cub/block/block_scan.cuh>
+// one thrust pass per clause, compacts per node and sorts the COO list by column.
+// Here one warp takes 32 states at a time (one bit per state in a 32-bit word): lane i
+// evaluates node i's rule over the 32 states, mostly by one look-up in a small table
+// of the rule over the state bits above 5 that it reads, a warp-wide 32 x 32 bit
+// transpose turns the node words into per-state flip masks, and the edges of a state
+// are emitted already sorted, so no sort is needed.
 #include <cub/device/device_scan.cuh>
 
 #include "esl_internal.h"
@@ -17,20 +18,21 @@
 namespace esl {
 namespace {
 
-constexpr int kMaskThreads = 128;                 // threads per block, one 32-state word each
-constexpr int kStatesPerBlock = kMaskThreads * 32;  // 4096 states per block
-constexpr int kEmitThreads = 256;
+constexpr int kMaskWarps = 8;                                           // warps per block
+constexpr int kWordsPerWarp = kTableBlockStates / 32 / kMaskWarps;      // 32-state words per warp
+constexpr int kEmitWarps = 8;
+constexpr int kEmitGroups = kTableBlockStates / 32 / kEmitWarps;        // 32-state groups per warp
 
 __constant__ uint32_t c_lowbit_pattern[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
 
 // Word of variable j over the 32 states 32*w + l (bit l = bit j of that state).
-__device__ __forceinline__ uint32_t var_word(int j, uint32_t w) {
+__device__ __forceinline__ uint32_t var_word(int j, uint64_t w) {
     return j < 5 ? c_lowbit_pattern[j] : (((w >> (j - 5)) & 1u) ? 0xFFFFFFFFu : 0u);
 }
 
 // DNF of node i over 32 states; `comp_self` evaluates it with bit i complemented
 // (the rule seen from the neighbour across bit i).
-__device__ __forceinline__ uint32_t eval_rule(const DevModel& m, int i, uint32_t w, bool comp_self) {
+__device__ __forceinline__ uint32_t eval_rule(const DevModel& m, int i, uint64_t w, bool comp_self) {
     uint32_t f = 0;
     for (int c = m.off[i]; c < m.off[i + 1]; c++) {
         uint32_t p = m.pos[c], q = m.neg[c];
@@ -54,143 +56,164 @@ __device__ __forceinline__ uint32_t eval_rule(const DevModel& m, int i, uint32_t
     return f;
 }
 
-// In-register transpose of a 32x32 bit matrix (a[r] bit c -> a[c] bit r):
-// at step j the bit-j halves of row and column index are exchanged.
-__device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
+// 32x32 bit transpose across a warp: lane r holds row r (bit c = column c) and gets
+// column r back (bit c = row c).  At step j the off-diagonal j x j blocks of every
+// 2j x 2j block are exchanged between lanes r and r ^ j.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t a, int lane) {
 #pragma unroll
-    for (int j = 16, k = 0; j != 0; j >>= 1, k++) {
+    for (int j = 16; j >= 1; j >>= 1) {
         const uint32_t m = (j == 16) ? 0x0000FFFFu : (j == 8) ? 0x00FF00FFu : (j == 4) ? 0x0F0F0F0Fu
-                                                   : (j == 2) ? 0x33333333u : 0x55555555u;
-#pragma unroll
-        for (int r = 0; r < 32; r++) {
-            if (r & j) continue;
-            uint32_t t = ((a[r] >> j) ^ a[r + j]) & m;
-            a[r] ^= t << j;
-            a[r + j] ^= t;
-        }
+                                                     : (j == 2) ? 0x33333333u : 0x55555555u;
+        const uint32_t b = __shfl_xor_sync(0xFFFFFFFFu, a, j);
+        if (lane & j)
+            a ^= ((b >> j) ^ a) & m;
+        else
+            a ^= (((a >> j) ^ b) & m) << j;
     }
+    return a;
 }
 
-// One thread per 32-state word: out-flip mask F and in-flip mask G per state, plus
-// the number of out-edges of the block.
-__global__ void __launch_bounds__(kMaskThreads) k_flip_masks(DevModel m, uint64_t n_words, uint64_t N,
-                                                             uint32_t* __restrict__ F, uint32_t* __restrict__ G,
-                                                             uint32_t* __restrict__ block_counts) {
-    __shared__ uint32_t s_tile[kMaskThreads * 33];
-    __shared__ uint32_t s_count;
-    const uint32_t w = blockIdx.x * kMaskThreads + threadIdx.x;
-    uint32_t fo[32], gi[32];
-#pragma unroll
-    for (int i = 0; i < 32; i++) {
-        fo[i] = 0;
-        gi[i] = 0;
-    }
-    if (threadIdx.x == 0) s_count = 0;
-    if (w < n_words) {
-#pragma unroll
-        for (int i = 0; i < 32; i++) {
-            if (i < m.n) {
-                const uint32_t x = var_word(i, w);
-                const uint32_t up = ((m.up_ok >> i) & 1u) ? 0xFFFFFFFFu : 0u;
-                const uint32_t dn = ((m.down_ok >> i) & 1u) ? 0xFFFFFFFFu : 0u;
-                const uint32_t f = eval_rule(m, i, w, false);
-                fo[i] = (f & ~x & up) | (~f & x & dn);
-                const uint32_t fc = ((m.self_dep >> i) & 1u) ? eval_rule(m, i, w, true) : f;
-                // neighbour u = s ^ (1<<i) has bit i = ~x; it flips i towards s when
-                // its rule (fc) equals s's bit, in the direction given by u's bit.
-                gi[i] = (fc & x & up) | (~fc & ~x & dn);
-            }
-        }
-    }
-    transpose32(fo);
-    transpose32(gi);
+// One warp per 32-state word, lane i = node i: the lane evaluates node i's rule over
+// the word's 32 states (from its rule table, else from the clauses), forms the words of
+// the up / down flips out of and into the 32 states, and a warp transpose turns the
+// n node words into the 32 per-state masks, stored coalesced.  A block covers
+// kTableBlockStates states and writes their out-edge count.
+__global__ void __launch_bounds__(kMaskWarps * 32) k_flip_masks(DevModel m, uint64_t n_words, uint64_t N,
+                                                                uint32_t* __restrict__ F, uint32_t* __restrict__ G,
+                                                                uint32_t* __restrict__ block_counts) {
+    extern __shared__ uint32_t s_tab[];
+    __shared__ uint4 s_info[32];
+    __shared__ uint32_t s_cnt[kMaskWarps];
+    for (uint32_t j = threadIdx.x; j < m.tab_words; j += blockDim.x) s_tab[j] = m.tab[j];
+    if (threadIdx.x < (unsigned)m.n) s_info[threadIdx.x] = m.info[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = lane;
+    const bool node = i < m.n;
+    const uint4 inf = node ? s_info[i] : make_uint4(0u, kNoRuleTable, 0u, 0u);
+    const uint32_t up = (node && ((m.up_ok >> i) & 1u)) ? 0xFFFFFFFFu : 0u;
+    const uint32_t dn = (node && ((m.down_ok >> i) & 1u)) ? 0xFFFFFFFFu : 0u;
+    const bool self = node && ((m.self_dep >> i) & 1u);
+    const uint32_t xlo = (node && i < 5) ? c_lowbit_pattern[i] : 0u;
     uint32_t cnt = 0;
-    const uint64_t base = (uint64_t)w * 32;
-#pragma unroll
-    for (int l = 0; l < 32; l++)
-        if (base + l < N) cnt += __popc(fo[l]);
-    __syncthreads();
-    atomicAdd(&s_count, cnt);
-    // coalesced stores through shared memory
-    const uint64_t blk_base = (uint64_t)blockIdx.x * kStatesPerBlock;
-#pragma unroll
-    for (int l = 0; l < 32; l++) s_tile[threadIdx.x * 33 + l] = fo[l];
-    __syncthreads();
-    for (int k = 0; k < 32; k++) {
-        int idx = k * kMaskThreads + threadIdx.x;
-        uint64_t s = blk_base + idx;
-        if (s < N) F[s] = s_tile[(idx >> 5) * 33 + (idx & 31)];
+    for (int j = 0; j < kWordsPerWarp; j++) {
+        const uint64_t w = (uint64_t)blockIdx.x * (kTableBlockStates / 32) + (uint64_t)warp * kWordsPerWarp + j;
+        if (w >= n_words) break;  // uniform over the warp
+        uint32_t fo = 0, gi = 0;
+        if (node) {
+            const uint32_t x = i < 5 ? xlo : (((w >> (i - 5)) & 1u) ? 0xFFFFFFFFu : 0u);
+            uint32_t f, fc;
+            if (inf.y != kNoRuleTable) {
+                uint32_t idx = 0;
+                for (uint32_t b = 0; b < inf.y; b++) {
+                    const uint32_t p = ((b < 4 ? inf.z : inf.w) >> (8 * (b & 3))) & 0xFFu;
+                    idx |= (uint32_t)((w >> p) & 1u) << b;
+                }
+                f = s_tab[inf.x + idx];
+                fc = self ? s_tab[inf.x + (1u << inf.y) + idx] : f;
+            } else {
+                f = eval_rule(m, i, w, false);
+                fc = (self && G) ? eval_rule(m, i, w, true) : f;
+            }
+            fo = (f & ~x & up) | (~f & x & dn);
+            // neighbour u = s ^ (1<<i) has bit i = ~x; it flips i towards s when its
+            // rule (fc) equals s's bit, in the direction given by u's bit.
+            gi = (fc & x & up) | (~fc & ~x & dn);
+        }
+        fo = warp_transpose32(fo, lane);
+        const uint64_t s = w * 32 + lane;
+        if (G) {
+            gi = warp_transpose32(gi, lane);
+            if (s < N) G[s] = gi;
+        }
+        if (s < N) {
+            F[s] = fo;
+            cnt += __popc(fo);
+        }
     }
-    __syncthreads();
 #pragma unroll
-    for (int l = 0; l < 32; l++) s_tile[threadIdx.x * 33 + l] = gi[l];
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    if (lane == 0) s_cnt[warp] = cnt;
     __syncthreads();
-    for (int k = 0; k < 32; k++) {
-        int idx = k * kMaskThreads + threadIdx.x;
-        uint64_t s = blk_base + idx;
-        if (s < N && G) G[s] = s_tile[(idx >> 5) * 33 + (idx & 31)];
+    if (threadIdx.x == 0 && block_counts) {
+        uint32_t tot = 0;
+        for (int k = 0; k < kMaskWarps; k++) tot += s_cnt[k];
+        block_counts[blockIdx.x] = tot;
     }
-    if (threadIdx.x == 0 && block_counts) block_counts[blockIdx.x] = s_count;
 }
 
-// CSC emission.  Block b covers the same 4096 states as block b of k_flip_masks and
-// starts writing edges at block_offsets[b].  Per 256-state chunk: degrees, block
-// scan, edges staged in shared memory in destination order, coalesced copy out.
+// CSC emission.  Block b covers the same kTableBlockStates states as block b of
+// k_flip_masks and starts writing edges at block_offsets[b]; each warp takes
+// kEmitGroups groups of 32 states, starts at the block offset plus the edges of the
+// warps before it, and per group: warp scan of the degrees, edges staged in the warp's
+// shared memory in destination order, coalesced copy out.  No block-wide barrier in the
+// loop.
 template <int MAXN>
-__global__ void __launch_bounds__(kEmitThreads) k_emit_csc(int n, uint64_t N, const uint32_t* __restrict__ F,
-                                                           const uint32_t* __restrict__ block_offsets,
-                                                           int32_t* __restrict__ indptr, int32_t* __restrict__ rows,
-                                                           int32_t* __restrict__ cols, int64_t nnz) {
-    using Scan = cub::BlockScan<uint32_t, kEmitThreads>;
-    __shared__ typename Scan::TempStorage s_scan;
-    // an edge is staged as (state within chunk, flipped bit): 2 bytes
-    __shared__ uint8_t s_loc[kEmitThreads * MAXN];
-    __shared__ uint8_t s_bit[kEmitThreads * MAXN];
-    __shared__ uint32_t s_total;
-    const uint64_t blk_base = (uint64_t)blockIdx.x * kStatesPerBlock;
+__global__ void __launch_bounds__(kEmitWarps * 32) k_emit_csc(int n, uint64_t N, const uint32_t* __restrict__ F,
+                                                             const uint32_t* __restrict__ block_offsets,
+                                                             int32_t* __restrict__ indptr, int32_t* __restrict__ rows,
+                                                             int32_t* __restrict__ cols, int64_t nnz) {
+    // an edge is staged as (state within the group << 5 | flipped bit)
+    __shared__ uint16_t s_stage[kEmitWarps][32 * MAXN];
+    __shared__ uint32_t s_wsum[kEmitWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t blk_base = (uint64_t)blockIdx.x * kTableBlockStates;
+    const uint64_t wbase = blk_base + (uint64_t)warp * 32 * kEmitGroups;
+    uint32_t f[kEmitGroups];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int g = 0; g < kEmitGroups; g++) {
+        const uint64_t s = wbase + (uint64_t)g * 32 + lane;
+        f[g] = s < N ? F[s] : 0u;
+        tot += __popc(f[g]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+    if (lane == 0) s_wsum[warp] = tot;
+    __syncthreads();
     uint64_t out = block_offsets[blockIdx.x];
-    for (int chunk = 0; chunk < kStatesPerBlock / kEmitThreads; chunk++) {
-        const uint64_t s = blk_base + (uint64_t)chunk * kEmitThreads + threadIdx.x;
-        if (blk_base + (uint64_t)chunk * kEmitThreads >= N) break;
-        const uint32_t f = s < N ? F[s] : 0u;
-        const uint32_t deg = __popc(f);
-        uint32_t excl, total;
-        Scan(s_scan).ExclusiveSum(deg, excl, total);
+    for (int k = 0; k < warp; k++) out += s_wsum[k];
+    uint16_t* st = s_stage[warp];
+#pragma unroll
+    for (int g = 0; g < kEmitGroups; g++) {
+        const uint64_t gb = wbase + (uint64_t)g * 32;
+        if (gb >= N) break;  // uniform over the warp
+        const uint32_t d = __popc(f[g]);
+        uint32_t incl = d;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t excl = incl - d;
+        const uint32_t gtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint64_t s = gb + lane;
         if (s < N) indptr[s] = (int32_t)(out + excl);
         // destinations ascending: clear bits high -> low, then set bits low -> high
         const uint32_t sv = (uint32_t)s;
-        uint32_t down = f & sv, up = f & ~sv;
-        int k = (int)excl;
+        uint32_t down = f[g] & sv, upm = f[g] & ~sv;
+        uint32_t k = excl;
         while (down) {
-            int i = 31 - __clz(down);
+            const int i = 31 - __clz(down);
             down &= ~(1u << i);
-            s_loc[k] = (uint8_t)threadIdx.x;
-            s_bit[k] = (uint8_t)i;
-            k++;
+            st[k++] = (uint16_t)((lane << 5) | i);
         }
-        while (up) {
-            int i = __ffs(up) - 1;
-            up &= up - 1;
-            s_loc[k] = (uint8_t)threadIdx.x;
-            s_bit[k] = (uint8_t)i;
-            k++;
+        while (upm) {
+            const int i = __ffs(upm) - 1;
+            upm &= upm - 1;
+            st[k++] = (uint16_t)((lane << 5) | i);
         }
-        if (threadIdx.x == 0) s_total = total;
-        __syncthreads();
-        const uint32_t tot = s_total;
-        const uint32_t chunk_base = (uint32_t)(blk_base + (uint64_t)chunk * kEmitThreads);
-        for (uint32_t e = threadIdx.x; e < tot; e += kEmitThreads) {
-            const uint32_t src = chunk_base + s_loc[e];
-            rows[out + e] = (int32_t)(src ^ (1u << s_bit[e]));
+        __syncwarp();
+        for (uint32_t e = lane; e < gtot; e += 32) {
+            const uint32_t v = st[e];
+            const uint32_t src = (uint32_t)gb + (v >> 5);
+            rows[out + e] = (int32_t)(src ^ (1u << (v & 31u)));
             if (cols) cols[out + e] = (int32_t)src;
         }
-        out += tot;
-        __syncthreads();
+        out += gtot;
+        __syncwarp();
     }
-    if (blk_base + kStatesPerBlock >= N && blk_base < N) {
-        // the block holding the last state closes indptr
-        if (threadIdx.x == 0) indptr[N] = (int32_t)nnz;
-    }
+    if (threadIdx.x == 0 && blk_base < N && blk_base + kTableBlockStates >= N) indptr[N] = (int32_t)nnz;
 }
 
 // Masks from an arbitrary CSC table whose every edge flips one bit.
@@ -223,70 +246,127 @@ __global__ void k_in_masks(int n, uint64_t N, const uint32_t* __restrict__ F, ui
 }  // namespace
 
 int64_t flip_mask_blocks(int n) {
-    uint64_t N = 1ull << n;
-    uint64_t words = (N + 31) / 32;
-    return (int64_t)((words + kMaskThreads - 1) / kMaskThreads);
+    const uint64_t N = 1ull << n;
+    return (int64_t)((N + kTableBlockStates - 1) / kTableBlockStates);
 }
 
-int upload_model(const Model& m, DevBuf<int32_t>& off, DevBuf<uint32_t>& pos, DevBuf<uint32_t>& neg,
-                 const double* rates, DevModel& dm, cudaStream_t s) {
-    int n = m.n();
-    std::vector<int32_t> h_off(n + 1, 0);
-    std::vector<uint32_t> h_pos, h_neg;
-    uint32_t self_dep = 0;
-    for (int i = 0; i < n; i++) {
-        for (const Clause& c : m.rules[i]) {
-            h_pos.push_back(c.pos);
-            h_neg.push_back(c.neg);
-            if (((c.pos | c.neg) >> i) & 1u) self_dep |= 1u << i;
+namespace {
+const uint32_t kLowPattern[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+
+// node i's DNF over the 32 states of word w (host form of eval_rule)
+uint32_t host_eval(const Model& m, int i, uint64_t w, bool comp_self) {
+    uint32_t f = 0;
+    for (const Clause& c : m.rules[i]) {
+        uint32_t t = 0xFFFFFFFFu;
+        for (int j = 0; j < 32; j++) {
+            const uint32_t b = 1u << j;
+            if (!((c.pos | c.neg) & b)) continue;
+            uint32_t x = j < 5 ? kLowPattern[j] : (((w >> (j - 5)) & 1u) ? 0xFFFFFFFFu : 0u);
+            if (comp_self && j == i) x = ~x;
+            t &= (c.pos & b) ? x : ~x;
         }
-        h_off[i + 1] = (int32_t)h_pos.size();
+        f |= t;
     }
-    ESL_TRY(off.alloc(h_off.size()));
-    ESL_TRY(pos.alloc(h_pos.size()));
-    ESL_TRY(neg.alloc(h_neg.size()));
-    ESL_CUDA(cudaMemcpyAsync(off.get(), h_off.data(), h_off.size() * 4, cudaMemcpyHostToDevice, s));
-    if (!h_pos.empty()) {
-        ESL_CUDA(cudaMemcpyAsync(pos.get(), h_pos.data(), h_pos.size() * 4, cudaMemcpyHostToDevice, s));
-        ESL_CUDA(cudaMemcpyAsync(neg.get(), h_neg.data(), h_neg.size() * 4, cudaMemcpyHostToDevice, s));
-    }
-    dm.n = n;
-    dm.off = off.get();
-    dm.pos = pos.get();
-    dm.neg = neg.get();
-    dm.up_ok = dm.down_ok = 0;
+    return f;
+}
+}  // namespace
+
+void host_model(const Model& m, HostModel& hm) {
+    const int n = m.n();
+    hm.off.assign(n + 1, 0);
+    hm.pos.clear();
+    hm.neg.clear();
+    hm.info.assign(n, make_uint4(0u, kNoRuleTable, 0u, 0u));
+    hm.tab.clear();
+    hm.self_dep = 0;
     for (int i = 0; i < n; i++) {
-        if (rates[2 * i] != 0.0) dm.up_ok |= 1u << i;
-        if (rates[2 * i + 1] != 0.0) dm.down_ok |= 1u << i;
+        uint32_t support = 0;
+        for (const Clause& c : m.rules[i]) {
+            hm.pos.push_back(c.pos);
+            hm.neg.push_back(c.neg);
+            support |= c.pos | c.neg;
+        }
+        hm.off[i + 1] = (int32_t)hm.pos.size();
+        if ((support >> i) & 1u) hm.self_dep |= 1u << i;
+        // the word bits (state bits >= 5) the rule reads
+        std::vector<uint32_t> hb;
+        for (int j = 5; j < 32; j++)
+            if ((support >> j) & 1u) hb.push_back((uint32_t)(j - 5));
+        const size_t words = (size_t)2 << hb.size();
+        if ((int)hb.size() > kRuleTableMaxBits || hm.tab.size() + words > (size_t)kRuleTableMaxWords) continue;
+        uint4 inf = make_uint4((uint32_t)hm.tab.size(), (uint32_t)hb.size(), 0u, 0u);
+        for (size_t b = 0; b < hb.size(); b++) (b < 4 ? inf.z : inf.w) |= hb[b] << (8 * (b & 3));
+        const uint32_t cnt = 1u << hb.size();
+        for (int comp = 0; comp < 2; comp++)
+            for (uint32_t a = 0; a < cnt; a++) {
+                uint64_t w = 0;
+                for (size_t b = 0; b < hb.size(); b++)
+                    if ((a >> b) & 1u) w |= 1ull << hb[b];
+                hm.tab.push_back(host_eval(m, i, w, comp != 0));
+            }
+        hm.info[i] = inf;
     }
-    dm.self_dep = self_dep;
+}
+
+void rate_masks(int n, const double* rates, uint32_t& up_ok, uint32_t& down_ok) {
+    up_ok = down_ok = 0;
+    for (int i = 0; i < n; i++) {
+        if (rates[2 * i] != 0.0) up_ok |= 1u << i;
+        if (rates[2 * i + 1] != 0.0) down_ok |= 1u << i;
+    }
+}
+
+int upload_model(const Model& m, DevModelBufs& b, const double* rates, DevModel& dm, cudaStream_t s) {
+    const int n = m.n();
+    HostModel hm;
+    host_model(m, hm);
+    ESL_TRY(b.off.alloc(hm.off.size()));
+    ESL_TRY(b.pos.alloc(hm.pos.size()));
+    ESL_TRY(b.neg.alloc(hm.neg.size()));
+    ESL_TRY(b.info.alloc(std::max<size_t>(hm.info.size(), 1)));
+    ESL_TRY(b.tab.alloc(hm.tab.size()));
+    ESL_CUDA(cudaMemcpyAsync(b.off.get(), hm.off.data(), hm.off.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!hm.pos.empty()) {
+        ESL_CUDA(cudaMemcpyAsync(b.pos.get(), hm.pos.data(), hm.pos.size() * 4, cudaMemcpyHostToDevice, s));
+        ESL_CUDA(cudaMemcpyAsync(b.neg.get(), hm.neg.data(), hm.neg.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    if (!hm.info.empty())
+        ESL_CUDA(cudaMemcpyAsync(b.info.get(), hm.info.data(), hm.info.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    if (!hm.tab.empty())
+        ESL_CUDA(cudaMemcpyAsync(b.tab.get(), hm.tab.data(), hm.tab.size() * 4, cudaMemcpyHostToDevice, s));
+    dm.n = n;
+    dm.off = b.off.get();
+    dm.pos = b.pos.get();
+    dm.neg = b.neg.get();
+    dm.info = b.info.get();
+    dm.tab = b.tab.get();
+    dm.tab_words = (uint32_t)hm.tab.size();
+    rate_masks(n, rates, dm.up_ok, dm.down_ok);
+    dm.self_dep = hm.self_dep;
     return ESL_OK;
 }
 
 int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* block_counts, cudaStream_t s) {
-    uint64_t N = 1ull << dm.n;
-    uint64_t words = (N + 31) / 32;
-    int64_t blocks = flip_mask_blocks(dm.n);
+    const uint64_t N = 1ull << dm.n;
+    const uint64_t words = (N + 31) / 32;
+    const int64_t blocks = flip_mask_blocks(dm.n);
     ESL_COUNT_LAUNCH();
-    k_flip_masks<<<(unsigned)blocks, kMaskThreads, 0, s>>>(dm, words, N, F, G, block_counts);
+    k_flip_masks<<<(unsigned)blocks, kMaskWarps * 32, (size_t)dm.tab_words * 4, s>>>(dm, words, N, F, G, block_counts);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
 }
 
 int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
                     int32_t* cols, int64_t nnz, cudaStream_t s) {
-    uint64_t N = 1ull << n;
-    int64_t blocks = flip_mask_blocks(n);
-    if (n <= 16) {
-        ESL_COUNT_LAUNCH();
-        k_emit_csc<16><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
-    } else if (n <= 24) {
-        ESL_COUNT_LAUNCH();
-        k_emit_csc<24><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
-    } else {
-        ESL_COUNT_LAUNCH();
-        k_emit_csc<30><<<(unsigned)blocks, kEmitThreads, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
-    }
+    const uint64_t N = 1ull << n;
+    const int64_t blocks = flip_mask_blocks(n);
+    ESL_COUNT_LAUNCH();
+    if (n <= 16)
+        k_emit_csc<16><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+    else if (n <= 24)
+        k_emit_csc<24><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+    else
+        k_emit_csc<30><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
 }

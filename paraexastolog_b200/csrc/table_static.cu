@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kStaticMaxNodes = ESL_STATIC_TABLE_MAX_NODES;
 constexpr size_t kStaticStates = (size_t)1 << kStaticMaxNodes;
-constexpr size_t kStaticBlocks = kStaticStates / 4096;  // flip-mask blocks cover 4096 states each
+constexpr size_t kStaticBlocks = kStaticStates / kTableBlockStates;  // count blocks of the table kernels
 constexpr size_t kStaticClauses = ESL_STATIC_TABLE_MAX_CLAUSES;
 constexpr size_t kScanTempBytes = 64 * 1024;
 // The CSC offsets are int32: at most n * 2^n edges must fit below 2^31.
@@ -41,7 +41,9 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kOffClauseOff = 0;
 constexpr size_t kOffPos = align256(kOffClauseOff + (ESL_MAX_NODES + 1) * sizeof(int32_t));
 constexpr size_t kOffNeg = align256(kOffPos + kStaticClauses * sizeof(uint32_t));
-constexpr size_t kOffF = align256(kOffNeg + kStaticClauses * sizeof(uint32_t));
+constexpr size_t kOffInfo = align256(kOffNeg + kStaticClauses * sizeof(uint32_t));
+constexpr size_t kOffTab = align256(kOffInfo + ESL_MAX_NODES * sizeof(uint4));
+constexpr size_t kOffF = align256(kOffTab + kRuleTableMaxWords * sizeof(uint32_t));
 constexpr size_t kOffCounts = align256(kOffF + kStaticStates * sizeof(uint32_t));
 constexpr size_t kOffOffsets = align256(kOffCounts + (kStaticBlocks + 1) * sizeof(uint32_t));
 constexpr size_t kOffScan = align256(kOffOffsets + (kStaticBlocks + 1) * sizeof(uint32_t));
@@ -93,21 +95,12 @@ extern "C" int esl_table_build_static(const esl_model* m, const double* rates, v
         if (!(rates[j] >= 0.0) || !std::isfinite(rates[j]))
             return fail(ESL_ERR_INVALID, "transition rate must be non-negative and finite");
 
-    // clause lists on the host (host memory only)
-    std::vector<int32_t> h_off(n + 1, 0);
-    std::vector<uint32_t> h_pos, h_neg;
-    uint32_t self_dep = 0;
-    for (int i = 0; i < n; i++) {
-        for (const Clause& c : model.rules[i]) {
-            h_pos.push_back(c.pos);
-            h_neg.push_back(c.neg);
-            if (((c.pos | c.neg) >> i) & 1u) self_dep |= 1u << i;
-        }
-        h_off[i + 1] = (int32_t)h_pos.size();
-    }
-    if (h_pos.size() > kStaticClauses)
+    // clause lists and rule tables on the host (host memory only)
+    HostModel hm;
+    host_model(model, hm);
+    if (hm.pos.size() > kStaticClauses)
         return fail(ESL_ERR_TOO_LARGE, "esl_table_build_static handles at most " + std::to_string(kStaticClauses) +
-                                           " DNF clauses; this model has " + std::to_string(h_pos.size()));
+                                           " DNF clauses; this model has " + std::to_string(hm.pos.size()));
 
     unsigned char* base = nullptr;
     ESL_TRY(scratch_for_current_device(&base));
@@ -115,27 +108,31 @@ extern "C" int esl_table_build_static(const esl_model* m, const double* rates, v
     int32_t* d_off = reinterpret_cast<int32_t*>(base + kOffClauseOff);
     uint32_t* d_pos = reinterpret_cast<uint32_t*>(base + kOffPos);
     uint32_t* d_neg = reinterpret_cast<uint32_t*>(base + kOffNeg);
+    uint4* d_info = reinterpret_cast<uint4*>(base + kOffInfo);
+    uint32_t* d_tab = reinterpret_cast<uint32_t*>(base + kOffTab);
     uint32_t* F = reinterpret_cast<uint32_t*>(base + kOffF);
     uint32_t* counts = reinterpret_cast<uint32_t*>(base + kOffCounts);
     uint32_t* offs = reinterpret_cast<uint32_t*>(base + kOffOffsets);
     void* scan_tmp = base + kOffScan;
 
-    ESL_CUDA(cudaMemcpyAsync(d_off, h_off.data(), h_off.size() * 4, cudaMemcpyHostToDevice, s));
-    if (!h_pos.empty()) {
-        ESL_CUDA(cudaMemcpyAsync(d_pos, h_pos.data(), h_pos.size() * 4, cudaMemcpyHostToDevice, s));
-        ESL_CUDA(cudaMemcpyAsync(d_neg, h_neg.data(), h_neg.size() * 4, cudaMemcpyHostToDevice, s));
+    ESL_CUDA(cudaMemcpyAsync(d_off, hm.off.data(), hm.off.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!hm.pos.empty()) {
+        ESL_CUDA(cudaMemcpyAsync(d_pos, hm.pos.data(), hm.pos.size() * 4, cudaMemcpyHostToDevice, s));
+        ESL_CUDA(cudaMemcpyAsync(d_neg, hm.neg.data(), hm.neg.size() * 4, cudaMemcpyHostToDevice, s));
     }
+    ESL_CUDA(cudaMemcpyAsync(d_info, hm.info.data(), hm.info.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    if (!hm.tab.empty())
+        ESL_CUDA(cudaMemcpyAsync(d_tab, hm.tab.data(), hm.tab.size() * 4, cudaMemcpyHostToDevice, s));
     DevModel dm;
     dm.n = n;
     dm.off = d_off;
     dm.pos = d_pos;
     dm.neg = d_neg;
-    dm.up_ok = dm.down_ok = 0;
-    for (int i = 0; i < n; i++) {
-        if (rates[2 * i] != 0.0) dm.up_ok |= 1u << i;
-        if (rates[2 * i + 1] != 0.0) dm.down_ok |= 1u << i;
-    }
-    dm.self_dep = self_dep;
+    dm.info = d_info;
+    dm.tab = d_tab;
+    dm.tab_words = (uint32_t)hm.tab.size();
+    rate_masks(n, rates, dm.up_ok, dm.down_ok);
+    dm.self_dep = hm.self_dep;
 
     // out-masks and per-block edge counts, then the edge total on the host
     ESL_TRY(launch_flip_masks(dm, F, nullptr, counts, s));
