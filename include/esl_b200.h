@@ -65,6 +65,8 @@ typedef struct esl_report {
     int refinements;       /* FP64 refinement steps taken */
     double relres;         /* final relative residual (max over the batch) */
     int converged;         /* 1 if every system met tol */
+    int fallback_systems;  /* systems the level sweep handed to the block forward solve */
+    int dense_lu_systems;  /* (system, level group) pairs solved by the dense LU of their SCC blocks */
 } esl_report;
 
 const char* esl_last_error(void);
@@ -74,6 +76,19 @@ int esl_version(void);
 int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out);
 int esl_ctx_destroy(esl_ctx* ctx);
 int esl_ctx_synchronize(esl_ctx* ctx);
+
+/* Budgets of the fallback paths (no counterpart in the reference, whose library calls
+ * std::exit on failure); a value <= 0 keeps the default.  Tests use them to drive every
+ * fallback branch without a device fault:
+ *   graph_sweeps: sweeps per fixpoint loop of the graph stages (default: 2^n + 64); past
+ *     it esl_net_build / esl_net_from_csc return ESL_ERR_TIMEOUT;
+ *   block_iters: Krylov iteration budget of the block forward solve, the fallback of
+ *     the level sweep (default max(esl_solve_opts.max_iters, 3000)); systems that miss
+ *     it get a dense FP64 LU of each SCC block of the level group;
+ *   dense_max: largest SCC block that dense LU takes (default 4096 states); a system
+ *     that misses the budget in a larger block returns ESL_ERR_NOT_CONVERGED.
+ * The context stays usable after any of these errors. */
+int esl_ctx_set_budgets(esl_ctx* ctx, int64_t graph_sweeps, int block_iters, int dense_max);
 
 /* ---- model: replaces model_builder::construct_model (cuda/src/model.cpp:80-125)
  *      and clause_t::get_positive_mask/get_negative_mask (cuda/src/model.cpp:8-21) */

@@ -46,7 +46,8 @@ class SolveOpts(C.Structure):
 
 
 class Report(C.Structure):
-    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("relres", C.c_double), ("converged", C.c_int)]
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("relres", C.c_double), ("converged", C.c_int),
+                ("fallback_systems", C.c_int), ("dense_lu_systems", C.c_int)]
 
 
 class Job(C.Structure):
@@ -74,6 +75,7 @@ def lib():
     L.esl_ctx_destroy.argtypes = [vp]
     L.esl_ctx_synchronize.argtypes = [vp]
     L.esl_ctx_set_profiling.argtypes = [vp, C.c_int]
+    L.esl_ctx_set_budgets.argtypes = [vp, C.c_int64, C.c_int, C.c_int]
     L.esl_launch_count.argtypes = [P(C.c_uint64)]
     L.esl_ctx_profile.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_int)]
     L.esl_ctx_profile_records.argtypes = [vp, C.c_int, vp, vp, P(C.c_int)]
@@ -183,6 +185,11 @@ class Context:
 
     def synchronize(self):
         check(lib().esl_ctx_synchronize(self._h))
+
+    def set_budgets(self, graph_sweeps: int = 0, block_iters: int = 0, dense_max: int = 0):
+        """Budgets of the fallback paths (0 keeps a default): sweeps per graph fixpoint
+        loop, Krylov iterations of the block forward solve, largest dense-LU block."""
+        check(lib().esl_ctx_set_budgets(self._h, int(graph_sweeps), int(block_iters), int(dense_max)))
 
     def set_profiling(self, on: bool):
         """Record CUDA events around each reduced-operator application of the solver."""

@@ -145,6 +145,14 @@ int esl_ctx_destroy(esl_ctx* c) {
     return ESL_OK;
 }
 
+int esl_ctx_set_budgets(esl_ctx* c, int64_t graph_sweeps, int block_iters, int dense_max) {
+    if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
+    c->graph_sweeps = graph_sweeps > 0 ? graph_sweeps : 0;
+    c->block_iters = block_iters > 0 ? block_iters : 0;
+    c->dense_max = dense_max > 0 ? dense_max : 0;
+    return ESL_OK;
+}
+
 int esl_ctx_set_profiling(esl_ctx* c, int on) {
     if (!c) return fail(ESL_ERR_INVALID, "ctx is NULL");
     ESL_CUDA(cudaStreamSynchronize(c->stream));

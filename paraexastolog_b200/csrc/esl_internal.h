@@ -121,6 +121,10 @@ struct esl_ctx {
     // level-sweep tiling of the last esl_net_autotune on this context (0 / -1: default),
     // used for networks that have no tuning of their own
     int tune_tile_mb = 0, tune_s2 = -1;
+    // budgets of the fallback paths (esl_ctx_set_budgets; 0: the default)
+    int64_t graph_sweeps = 0;   // sweeps per fixpoint loop of the graph stages
+    int block_iters = 0;        // Krylov budget of the block forward solve
+    int dense_max = 0;          // largest SCC block of the dense LU fallback
     // measurement hook: events around the launches of the hot kernels, each record
     // with its kernel class and algorithmic bytes
     bool prof = false;

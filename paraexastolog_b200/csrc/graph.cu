@@ -276,8 +276,8 @@ int build_graph(esl_ctx* ctx, esl_net* net) {
     auto ms_since = [&]() {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
-    // budgets: a sweep can only fail to progress once per state
-    const int64_t budget = (int64_t)N + 64;
+    // budgets: a sweep can only fail to progress once per state (or the context's budget)
+    const int64_t budget = ctx->graph_sweeps > 0 ? ctx->graph_sweeps : (int64_t)N + 64;
     // nominal algorithmic bytes of one fixpoint sweep (measurement hook): one pass over
     // every state's mask, label and colour / level word, 4 B each.  States already
     // assigned read only their label, so later sweeps move less than this.

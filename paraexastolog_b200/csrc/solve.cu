@@ -68,6 +68,13 @@ constexpr double kAcceptRel = 1e-8;
 // by dense LU instead
 constexpr int kBlockBudget = 3000;
 constexpr int kDenseFallbackMax = 4096;
+// scratch of one dense-fallback launch; failed systems are taken in chunks that fit
+constexpr size_t kDenseScratchBytes = (size_t)2 << 30;
+
+int block_budget(const esl_ctx* ctx, const esl_solve_opts& o) {
+    return ctx->block_iters > 0 ? ctx->block_iters : std::max(o.max_iters, kBlockBudget);
+}
+int dense_cap(const esl_ctx* ctx) { return ctx->dense_max > 0 ? ctx->dense_max : kDenseFallbackMax; }
 
 template <class T>
 __device__ __forceinline__ void load_rates(T* s_rate, const double* __restrict__ rates, int b, int n) {
@@ -960,7 +967,19 @@ struct SolveOut {
     double relres = 0.0;
     bool converged = true;
     std::vector<double> sys_relres;  // per system, from the last Krylov solve
+    int fallback_systems = 0;        // systems the level sweep handed to the block forward solve
+    int dense_systems = 0;           // (system, level group) pairs solved by the dense LU fallback
 };
+
+void fill_report(esl_report* rep, const SolveOut& agg, bool converged) {
+    if (!rep) return;
+    rep->iterations = agg.iters;
+    rep->refinements = agg.refinements;
+    rep->relres = agg.relres;
+    rep->converged = converged ? 1 : 0;
+    rep->fallback_systems = agg.fallback_systems;
+    rep->dense_lu_systems = agg.dense_systems;
+}
 
 // Solves the K systems whose rhs halves are in (bE, bO); solution in x64 (odd) and zE (even).
 template <bool FWD>
@@ -1486,7 +1505,7 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
                 if (so.sys_relres[k] > kAcceptRel) failed.push_back(k);
                 else worst = std::max(worst, so.sys_relres[k]);
             const int nscc = (int)(P->off_scc[gi + 1] - P->off_scc[gi]);
-            const bool covered = P->max_scc[gi] <= kDenseFallbackMax;
+            const bool covered = P->max_scc[gi] <= dense_cap(ctx);
             if (!covered || nscc == 0) {
                 out.converged = false;
                 worst = so.relres;
@@ -1501,17 +1520,25 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
                     ESL_CUDA(cudaStreamSynchronize(s));
                     acc += sz * (sz + 1);
                 }
+                // systems in chunks whose matrices fit the scratch budget
+                const int chunk = (int)std::max<int64_t>(
+                    1, std::min<int64_t>(Kf, (int64_t)(kDenseScratchBytes / (8 * (size_t)std::max<int64_t>(acc, 1)))));
                 int64_t* d_scr = (int64_t*)ws.get(S_LUOFF, (size_t)nscc * 8, &st_);
                 int32_t* d_sys = (int32_t*)ws.get(S_LUSYS, (size_t)Kf * 4, &st_);
-                double* scratch = (double*)ws.get(S_LU, (size_t)acc * Kf * 8, &st_);
+                double* scratch = (double*)ws.get(S_LU, (size_t)acc * chunk * 8, &st_);
                 if (st_ != ESL_OK) return st_;
                 ESL_CUDA(cudaMemcpyAsync(d_scr, scr.data(), (size_t)nscc * 8, cudaMemcpyHostToDevice, s));
                 ESL_CUDA(cudaMemcpyAsync(d_sys, failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
-                ESL_COUNT_LAUNCH();
-                k_dense_block<<<dim3((unsigned)nscc, (unsigned)Kf), 256, 0, s>>>(
-                    net->n, P->scc_beg.get() + P->off_scc[gi], P->scc_size.get() + P->off_scc[gi], d_scr, d_sys, acc,
-                    net->order.get(), net->F.get(), net->G.get(), rates, nrhs, L.ld, bE, bO, ZE, ZO, scratch);
-                ESL_CUDA(cudaGetLastError());
+                out.dense_systems += Kf;
+                for (int c0 = 0; c0 < Kf; c0 += chunk) {
+                    const int kc = std::min(chunk, Kf - c0);
+                    ESL_COUNT_LAUNCH();
+                    k_dense_block<<<dim3((unsigned)nscc, (unsigned)kc), 256, 0, s>>>(
+                        net->n, P->scc_beg.get() + P->off_scc[gi], P->scc_size.get() + P->off_scc[gi], d_scr,
+                        d_sys + c0, acc, net->order.get(), net->F.get(), net->G.get(), rates, nrhs, L.ld, bE, bO, ZE,
+                        ZO, scratch);
+                    ESL_CUDA(cudaGetLastError());
+                }
                 ESL_CUDA(cudaStreamSynchronize(s));
                 if (debug_enabled())
                     fprintf(stderr, "[esl] group %d: dense LU fallback for %d systems on %d SCC blocks\n", gi, Kf, nscc);
@@ -1683,10 +1710,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             agg.relres = std::max(agg.relres, sw.relres);
             if (rc != ESL_OK) {
                 if (rep) {
-                    rep->iterations = agg.iters;
-                    rep->refinements = agg.refinements;
-                    rep->relres = agg.relres;
-                    rep->converged = 0;
+                    fill_report(rep, agg, false);
                 }
                 return rc;
             }
@@ -1784,11 +1808,14 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             esl_solve_opts bo = o;
             bo.method = ESL_METHOD_DIRECT;
             bo.d_warm = nullptr;
-            bo.max_iters = std::max(o.max_iters, kBlockBudget);
+            bo.max_iters = block_budget(ctx, o);
+            bo.max_refine = std::max(o.max_refine, 6);  // the fallback refines at least as far as the default
             SolveOut sb;
             rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
             if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
             agg.iters += sb.iters;
+            agg.fallback_systems += Kf;
+            agg.dense_systems += sb.dense_systems;
             agg.converged = sb.converged;
             agg.relres = std::max(agg.relres, sb.relres);
             ESL_CUDA(cudaMemsetAsync(y_sub, 0, (size_t)Kf * T * 8, s));
@@ -1801,10 +1828,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ESL_CUDA(cudaGetLastError());
             if (rc == ESL_ERR_NOT_CONVERGED) {
                 if (rep) {
-                    rep->iterations = agg.iters;
-                    rep->refinements = agg.refinements;
-                    rep->relres = agg.relres;
-                    rep->converged = 0;
+                    fill_report(rep, agg, false);
                 }
                 return rc;
             }
@@ -1828,9 +1852,10 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             ZO = (double*)ws.get(S_ZOF, vec * 8, &st_);
             if (st_ != ESL_OK) return st_;
             esl_solve_opts bo = o;
-            bo.max_iters = std::max(o.max_iters, kBlockBudget);
+            bo.max_iters = block_budget(ctx, o);
             rc = block_forward_solve(ctx, ws, net, K, R, d_rates, d_x0, N, ZE, ZO, bo, so);
             agg.iters += so.iters;
+            agg.dense_systems += so.dense_systems;
             agg.relres = so.relres;
             agg.converged = so.converged;
         } else {
@@ -1874,10 +1899,13 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
                 }
                 ESL_CUDA(cudaMemcpyAsync(d_failed, failed.data(), (size_t)Kf * 4, cudaMemcpyHostToDevice, s));
                 esl_solve_opts bo = o;
-                bo.max_iters = std::max(o.max_iters, kBlockBudget);
+                bo.max_iters = block_budget(ctx, o);
+                bo.max_refine = std::max(o.max_refine, 6);
                 SolveOut sb;
                 rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
                 agg.iters += sb.iters;
+                agg.fallback_systems += Kf;
+                agg.dense_systems += sb.dense_systems;
                 agg.converged = sb.converged;
                 double worst = 0.0;
                 for (int k = 0; k < K; k++)
@@ -1899,10 +1927,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         ESL_CUDA(cudaGetLastError());
         if (rc == ESL_ERR_NOT_CONVERGED) {
             if (rep) {
-                rep->iterations = agg.iters;
-                rep->refinements = agg.refinements;
-                rep->relres = agg.relres;
-                rep->converged = 0;
+                fill_report(rep, agg, false);
             }
             return rc;
         }
@@ -1967,10 +1992,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     }
     ESL_CUDA(cudaStreamSynchronize(s));
     if (rep) {
-        rep->iterations = agg.iters;
-        rep->refinements = agg.refinements;
-        rep->relres = agg.relres;
-        rep->converged = agg.converged ? 1 : 0;
+        fill_report(rep, agg, agg.converged);
     }
     return ESL_OK;
 }

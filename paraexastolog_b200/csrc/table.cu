@@ -95,20 +95,29 @@ __global__ void __launch_bounds__(kMaskWarps * 32) k_flip_masks(DevModel m, uint
     const uint32_t dn = (node && ((m.down_ok >> i) & 1u)) ? 0xFFFFFFFFu : 0u;
     const bool self = node && ((m.self_dep >> i) & 1u);
     const uint32_t xlo = (node && i < 5) ? c_lowbit_pattern[i] : 0u;
+    // The warp's words w0 .. w0 + 3 differ only in their two low bits: the table index
+    // is idx0 (from w0) plus the table bits at word bits 0 and 1 (lo0, lo1) as set in j.
+    const uint64_t w0 = (uint64_t)blockIdx.x * (kTableBlockStates / 32) + (uint64_t)warp * kWordsPerWarp;
+    static_assert(kWordsPerWarp == 4, "the index split assumes 4 words per warp");
+    uint32_t idx0 = 0, lo0 = 0, lo1 = 0;
+    if (node && inf.y != kNoRuleTable) {
+        for (uint32_t b = 0; b < inf.y; b++) {
+            const uint32_t p = ((b < 4 ? inf.z : inf.w) >> (8 * (b & 3))) & 0xFFu;
+            idx0 |= (uint32_t)((w0 >> p) & 1u) << b;
+            if (p == 0) lo0 = 1u << b;
+            if (p == 1) lo1 = 1u << b;
+        }
+    }
     uint32_t cnt = 0;
     for (int j = 0; j < kWordsPerWarp; j++) {
-        const uint64_t w = (uint64_t)blockIdx.x * (kTableBlockStates / 32) + (uint64_t)warp * kWordsPerWarp + j;
+        const uint64_t w = w0 + j;
         if (w >= n_words) break;  // uniform over the warp
         uint32_t fo = 0, gi = 0;
         if (node) {
             const uint32_t x = i < 5 ? xlo : (((w >> (i - 5)) & 1u) ? 0xFFFFFFFFu : 0u);
             uint32_t f, fc;
             if (inf.y != kNoRuleTable) {
-                uint32_t idx = 0;
-                for (uint32_t b = 0; b < inf.y; b++) {
-                    const uint32_t p = ((b < 4 ? inf.z : inf.w) >> (8 * (b & 3))) & 0xFFu;
-                    idx |= (uint32_t)((w >> p) & 1u) << b;
-                }
+                const uint32_t idx = idx0 | ((j & 1) ? lo0 : 0u) | ((j & 2) ? lo1 : 0u);
                 f = s_tab[inf.x + idx];
                 fc = self ? s_tab[inf.x + (1u << inf.y) + idx] : f;
             } else {
