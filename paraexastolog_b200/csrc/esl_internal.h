@@ -266,7 +266,7 @@ constexpr int kDenseTerminalMax = 128;
 // x0 row k % nrhs).  Systems that miss the tolerance are listed in `failed` (their y
 // rows are left as computed) and the call returns ESL_ERR_NOT_CONVERGED.
 struct SweepStats {
-    int iters = 0, refinements = 0, local_groups = 0, krylov_groups = 0;
+    int iters = 0, refinements = 0, local_groups = 0, krylov_groups = 0, compactions = 0;
     double relres = 0.0;
     std::vector<int32_t> failed;
 };

@@ -134,6 +134,8 @@ struct Layout {
     uint32_t H;         // half length N/2
     size_t ld;          // leading dimension of per-system vectors
     int nrhs;           // systems per rate set
+    // x0 row of system k: k % nrhs, or k when the caller gathered one x0 row per system
+    int x0_sys = 0;
     const uint32_t* M0; // even-half coupling masks | domain bit
     const uint32_t* M1; // odd-half coupling masks | domain bit
     const uint32_t* F0; // even-half out-masks
@@ -529,14 +531,16 @@ __global__ void k_rhs(Layout L, int n, const double* __restrict__ rates, const d
 
 // ---- assembly ---------------------------------------------------------------------
 // forward: y[k][t] += x0(v) + sum_{u -> v, u transient} rate * z(u) over v in t
-__global__ void k_terminal_mass(int n, int T, int term_states, int nrhs, size_t ld, const double* __restrict__ rates,
+// x0_sys: x0 row of system k is k (one gathered row per system) instead of k % nrhs.
+__global__ void k_terminal_mass(int n, int T, int term_states, int nrhs, int x0_sys, size_t ld,
+                                const double* __restrict__ rates,
                                 const double* __restrict__ x0, size_t x0_ld, const int32_t* __restrict__ order,
                                 const int32_t* __restrict__ term_of, const uint32_t* __restrict__ G,
                                 const double* __restrict__ zE, const double* __restrict__ zO,
                                 double* __restrict__ y) {
     const int k = blockIdx.y;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = k / nrhs, r = k % nrhs;
+    const int b = k / nrhs, r = x0_sys ? k : k % nrhs;
     const double* rt = rates + (size_t)b * 2 * n;
     int t = -1;
     double acc = 0.0;
@@ -1395,7 +1399,7 @@ __global__ void __launch_bounds__(kT) k_group_rhs(Layout L, int parity, const do
     if (!row_h(L, parity, h)) return;
     const uint32_t v = state_of(h, parity);
     const size_t o = (size_t)k * L.ld;
-    double acc = x0[(size_t)(k % L.nrhs) * x0_ld + v];
+    double acc = x0[(size_t)(L.x0_sys ? k : k % L.nrhs) * x0_ld + v];
     uint32_t g = Gx[v];
     while (g) {
         int i = __ffs(g) - 1;
@@ -1439,9 +1443,10 @@ __global__ void k_scatter_systems(size_t ld, const int32_t* __restrict__ idx, co
 
 // Block forward solve of K systems (rate set k / nrhs, x0 row k % nrhs); results in
 // the half-layout arrays ZE (even) and ZO (odd).
+// x0_per_system: x0 holds one row per system (a gathered subset) instead of nrhs rows.
 int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, int nrhs, const double* rates,
                         const double* x0, size_t x0_ld, double* ZE, double* ZO, const esl_solve_opts& o,
-                        SolveOut& out) {
+                        SolveOut& out, bool x0_per_system = false) {
     cudaStream_t s = ctx->stream;
     BlockPlan* P = nullptr;
     ESL_TRY(get_plan(ctx, net, P));
@@ -1451,6 +1456,7 @@ int block_forward_solve(esl_ctx* ctx, Workspace& ws, const esl_net* net, int K, 
     L.H = H;
     L.ld = ((size_t)H + 31) & ~(size_t)31;
     L.nrhs = nrhs;
+    L.x0_sys = x0_per_system ? 1 : 0;
     L.M0 = P->hm.get();
     L.M1 = P->hm.get() + H;
     L.F0 = P->hm.get() + 2 * (size_t)H;
@@ -1811,7 +1817,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             bo.max_iters = block_budget(ctx, o);
             bo.max_refine = std::max(o.max_refine, 6);  // the fallback refines at least as far as the default
             SolveOut sb;
-            rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
+            rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb, true);
             if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
             agg.iters += sb.iters;
             agg.fallback_systems += Kf;
@@ -1820,7 +1826,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             agg.relres = std::max(agg.relres, sb.relres);
             ESL_CUDA(cudaMemsetAsync(y_sub, 0, (size_t)Kf * T * 8, s));
             ESL_COUNT_LAUNCH();
-            k_terminal_mass<<<dim3((TS + 127) / 128, Kf), 128, 0, s>>>(n, T, TS, 1, L.ld, r_sub, x_sub, N,
+            k_terminal_mass<<<dim3((TS + 127) / 128, Kf), 128, 0, s>>>(n, T, TS, 1, 1, L.ld, r_sub, x_sub, N,
                                                                          net->order.get(), net->term_of.get(),
                                                                          net->G.get(), ZEb, ZOb, y_sub);
             ESL_COUNT_LAUNCH();
@@ -1902,7 +1908,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
                 bo.max_iters = block_budget(ctx, o);
                 bo.max_refine = std::max(o.max_refine, 6);
                 SolveOut sb;
-                rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb);
+                rc = block_forward_solve(ctx, ws, net, Kf, 1, r_sub, x_sub, N, ZEb, ZOb, bo, sb, true);
                 agg.iters += sb.iters;
                 agg.fallback_systems += Kf;
                 agg.dense_systems += sb.dense_systems;
@@ -1921,7 +1927,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
         }
         if (rc != ESL_OK && rc != ESL_ERR_NOT_CONVERGED) return rc;
         ESL_COUNT_LAUNCH();
-        k_terminal_mass<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, L.ld, d_rates, d_x0, N,
+        k_terminal_mass<<<dim3((TS + 127) / 128, K), 128, 0, s>>>(n, T, TS, R, 0, L.ld, d_rates, d_x0, N,
                                                                     net->order.get(), net->term_of.get(),
                                                                     net->G.get(), ZE, ZO, y);
         ESL_CUDA(cudaGetLastError());
@@ -1934,7 +1940,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
     } else {
         dim3 g((TS + 127) / 128, K);
         ESL_COUNT_LAUNCH();
-        k_terminal_mass<<<g, 128, 0, s>>>(n, T, TS, R, 0, d_rates, d_x0, N, net->order.get(), net->term_of.get(),
+        k_terminal_mass<<<g, 128, 0, s>>>(n, T, TS, R, 0, 0, d_rates, d_x0, N, net->order.get(), net->term_of.get(),
                                           net->G.get(), nullptr, nullptr, y);
         ESL_CUDA(cudaGetLastError());
     }

@@ -620,6 +620,114 @@ __global__ void k_sw_term_norm(int K, int TS, uint32_t p0, uint32_t count, const
         Rb[(size_t)k * TS + p0 + i] *= inv;
 }
 
+// ---- compaction of running systems --------------------------------------------------------
+// A system tile runs until its slowest system stops, so once the running systems fit in
+// fewer tiles they are moved to the leading columns of every per-system array (a
+// physical permutation of each row's system run, so that the kernels keep their
+// coalesced [row][system] access) and the grid shrinks.  cperm maps the compacted
+// column to the original system; the inverse permutation restores every array before
+// the inner solve's result is committed.
+constexpr int kCompactMaxKp = 1024;  // a row's systems are permuted in shared memory
+constexpr int kPermWarps = 4;
+
+__device__ __forceinline__ bool sw_running(int f) { return (f & SW_RUN) && !(f & SW_IDONE); }
+
+__global__ void k_sw_iota(int n, int* __restrict__ p) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) p[k] = k;
+}
+
+// Stable partition of the columns [0, Kc): running systems first.  p2[new] = old column;
+// cperm[new] = cperm[old].  One CTA.
+__global__ void __launch_bounds__(1024) k_sw_perm_build(int Kc, const int* __restrict__ flags, int* __restrict__ cperm,
+                                                        int* __restrict__ p2) {
+    __shared__ int s_run[kCompactMaxKp / 32 + 1], s_stop[kCompactMaxKp / 32 + 1];
+    __shared__ int s_old[kCompactMaxKp];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nch = (Kc + 31) / 32;
+    for (int k = threadIdx.x; k < Kc; k += blockDim.x) s_old[k] = cperm[k];
+    for (int c = warp; c < nch; c += nw) {
+        const int k = c * 32 + lane;
+        const bool valid = k < Kc;
+        const bool run = valid && sw_running(flags[k]);
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, run), v = __ballot_sync(0xFFFFFFFFu, valid);
+        if (lane == 0) {
+            s_run[c] = __popc(m);
+            s_stop[c] = __popc(v & ~m);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ra = 0, sa = 0;
+        for (int c = 0; c < nch; c++) {
+            const int r = s_run[c], q = s_stop[c];
+            s_run[c] = ra;
+            s_stop[c] = sa;
+            ra += r;
+            sa += q;
+        }
+        s_run[nch] = ra;
+    }
+    __syncthreads();
+    const int total = s_run[nch];
+    for (int c = warp; c < nch; c += nw) {
+        const int k = c * 32 + lane;
+        const bool valid = k < Kc;
+        const bool run = valid && sw_running(flags[k]);
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, run), v = __ballot_sync(0xFFFFFFFFu, valid);
+        const unsigned lt = (1u << lane) - 1u;
+        if (valid) {
+            const int pos = run ? s_run[c] + __popc(m & lt) : total + s_stop[c] + __popc(v & ~m & lt);
+            p2[pos] = k;
+            cperm[pos] = s_old[k];
+        }
+    }
+}
+
+struct PermArr {
+    void* p;
+    uint32_t rows;
+    int esize;  // 4 or 8 bytes
+};
+struct PermList {
+    PermArr a[16];
+};
+
+// Array blockIdx.y, each of its rows (stride Kp): forward row[k] = row_old[p[k]], inverse
+// row[p[k]] = row_old[k], for k < Kc.  One warp per row, the row staged in shared memory.
+__global__ void __launch_bounds__(kPermWarps * 32) k_sw_row_perm(PermList L, int Kp, int Kc, const int* __restrict__ p,
+                                                                 int inverse) {
+    extern __shared__ double s_rowbuf[];
+    const PermArr A = L.a[blockIdx.y];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* sm = s_rowbuf + (size_t)warp * Kc;
+    for (uint32_t r = blockIdx.x * kPermWarps + warp; r < A.rows; r += gridDim.x * kPermWarps) {
+        if (A.esize == 8) {
+            double* row = static_cast<double*>(A.p) + (size_t)r * Kp;
+            for (int k = lane; k < Kc; k += 32) sm[k] = row[k];
+            __syncwarp();
+            for (int k = lane; k < Kc; k += 32) {
+                if (inverse)
+                    row[p[k]] = sm[k];
+                else
+                    row[k] = sm[p[k]];
+            }
+        } else {
+            float* row = static_cast<float*>(A.p) + (size_t)r * Kp;
+            float* sf = reinterpret_cast<float*>(sm);
+            for (int k = lane; k < Kc; k += 32) sf[k] = row[k];
+            __syncwarp();
+            for (int k = lane; k < Kc; k += 32) {
+                if (inverse)
+                    row[p[k]] = sf[k];
+                else
+                    row[k] = sf[p[k]];
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ---- BiCGStab vector steps (odd rows; scalars per system) --------------------------------
 struct SwScalPtr {
     double* c[C_NSCAL];
@@ -726,8 +834,15 @@ __global__ void k_sw_outer(int K, SwScalPtr sc, double tol2, double inner_rel2, 
             continue;
         }
         if (outer > 0 && !(rr < 0.25 * sc.c[C_PREV][k])) sc.i[I_NOIMP][k]++;
-        if (sc.i[I_NOIMP][k] >= 2 || outer >= max_refine || !isfinite(rr)) {
+        // A system whose refinement stagnates has reached what FP64 delivers for it and
+        // is accepted within the acceptance residual; one that runs out of refinement
+        // steps while still improving has missed its budget and goes to the fallback.
+        if (sc.i[I_NOIMP][k] >= 2 || !isfinite(rr)) {
             sc.i[I_FLAGS][k] = (rr <= accept2 * b2) ? SW_DONE : (SW_DONE | SW_FAIL);
+            continue;
+        }
+        if (outer >= max_refine) {
+            sc.i[I_FLAGS][k] = SW_DONE | SW_FAIL;
             continue;
         }
         // the inner solve works on the residual scaled to unit norm
@@ -1077,9 +1192,14 @@ __global__ void __launch_bounds__(kSwLocalWarps * 32) k_sw_local(SwArgs a, SwLoc
             } else {
                 if (stepped && last32 && !(rr < 0.25 * prev)) use64 = true;
                 if (stepped && !last32 && !(rr < 0.25 * prev)) noimp++;
-                if (noimp >= 2 || outer >= l.max_refine + 3 || !isfinite(rr)) {
+                if (noimp >= 2 || !isfinite(rr)) {
+                    // stagnation: accepted within the acceptance residual
                     done = true;
                     failed = !(rr <= l.accept2 * b2);
+                } else if (outer >= l.max_refine + 3) {
+                    // out of refinement steps while still improving: the fallback redoes it
+                    done = true;
+                    failed = true;
                 }
             }
         }
@@ -1176,7 +1296,7 @@ __global__ void k_sw_rate_table(int n, int K, int Kp, int nrhs, const double* __
 
 // ---- host side ------------------------------------------------------------------------------
 enum SwSlot { W_Z, W_RATET, W_BV, W_BS, W_R64, W_DS64, W_DS32, W_W64, W_WT, W_R, W_R0, W_PH, W_V, W_SH, W_TT,
-              W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_QO, W_IQE, W_F0, W_COUNT = W_F0 + 8 };
+              W_D, W_SCAL, W_ISCAL, W_CNT, W_LOC, W_QO, W_IQE, W_PERM, W_F0, W_COUNT = W_F0 + 8 };
 
 bool debug_on();
 
@@ -1514,16 +1634,30 @@ struct GraphPair {
     GraphPair() = default;
     GraphPair(const GraphPair&) = delete;
     GraphPair& operator=(const GraphPair&) = delete;
-    ~GraphPair() {
+    void reset() {
         for (int p = 0; p < 2; p++) {
             if (exec[p]) cudaGraphExecDestroy(exec[p]);
             if (graph[p]) cudaGraphDestroy(graph[p]);
+            exec[p] = nullptr;
+            graph[p] = nullptr;
         }
     }
+    ~GraphPair() { reset(); }
 };
 
 bool debug_on() {
     static const bool on = getenv("ESL_DEBUG") != nullptr;
+    return on;
+}
+
+// Compaction of running systems in the grid-wide groups (ESL_SWEEP_COMPACT=0 turns it
+// off); groups under kCompactMinRows rows are launch-bound and keep their grid.
+constexpr uint32_t kCompactMinRows = 4096;
+bool compact_on() {
+    static const bool on = [] {
+        const char* e = getenv("ESL_SWEEP_COMPACT");
+        return !(e && e[0] == '0');
+    }();
     return on;
 }
 
@@ -1824,12 +1958,11 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
             a.flags = sc.i[I_FLAGS];
             a.KT = inner64 ? gKT64 : gKT32;
             const size_t smT = inner64 ? gsm64 : gsm32;
-            const dim3 gei = row_grid(g.ne, Kp, a.KT, ctx->sm_count), goi = row_grid(g.no, Kp, a.KT, ctx->sm_count);
+            dim3 gei = row_grid(g.ne, Kp, a.KT, ctx->sm_count), goi = row_grid(g.no, Kp, a.KT, ctx->sm_count);
             // two systems per thread in the gather kernels when the tile is wide enough
             // (not in deflated groups)
             const bool s2 = !defl && a.KT >= 64 && (net->tune_s2 >= 0 ? net->tune_s2 != 0 : ctx->tune_s2 != 0);
-            const dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2),
-                       goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
+            dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2), goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
             auto run_inner = [&](auto tag) -> int {
                 using TT = decltype(tag);
                 TT* R = (TT*)vR;
@@ -1885,7 +2018,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                         ESL_COUNT_LAUNCH();
                         k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                         ESL_COUNT_LAUNCH();
-                        k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
+                        k_sw_scal<<<1, 1024, 0, s>>>(a.K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
                                                      d_cnt + 1 + par);
                         }
                         continue;
@@ -1929,12 +2062,26 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                         k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                     }
                     ESL_COUNT_LAUNCH();
-                    k_sw_scal<<<1, 1024, 0, s>>>(K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
+                    k_sw_scal<<<1, 1024, 0, s>>>(a.K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
                                                  d_cnt + 1 + par);
                     }
                     ESL_CUDA(cudaGetLastError());
                     return ESL_OK;
                 };
+                // compaction state: Kc leading columns hold the systems that may still run
+                const bool can_compact = compact_on() && Kp <= kCompactMaxKp && (g.ne + g.no) >= kCompactMinRows;
+                int Kc = Kp;
+                bool compacted = false;
+                int *cperm = nullptr, *p2 = nullptr;
+                PermList pl{};
+                int npl = 0;
+                auto add_perm = [&](const void* p, uint32_t nrows, int es) {
+                    if (p && nrows) pl.a[npl++] = PermArr{const_cast<void*>(p), nrows, es};
+                };
+                const dim3 gei0 = gei, goi0 = goi, gei20 = gei2, goi20 = goi2;
+                const unsigned perm_blocks = (unsigned)std::max<uint64_t>(
+                    1, std::min<uint64_t>(((uint64_t)std::max(g.ne, g.no) + kPermWarps - 1) / kPermWarps,
+                                          (uint64_t)ctx->sm_count * 8));
                 // After the first poll window the launches of a window are replayed from a
                 // CUDA graph (one per slot parity): the small level groups are bound by the
                 // host's launch rate, not by the GPU.
@@ -1972,11 +2119,66 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                     ESL_CUDA(cudaEventRecord(ctx->poll_ev[chunk & 1], s));
                     if (chunk >= 1) {
                         ESL_CUDA(cudaEventSynchronize(ctx->poll_ev[(chunk - 1) & 1]));
-                        if (h_cnt[1 + ((chunk - 1) & 1)] == 0) {
+                        const int nr = h_cnt[1 + ((chunk - 1) & 1)];
+                        if (nr == 0) {
                             it += kSwPoll;
                             break;
                         }
+                        // The count is that of the window before the one in flight, an upper
+                        // bound of the systems still running when the compaction (queued
+                        // behind that window) runs.
+                        const int tiles_now = Kc / a.KT, tiles_new = (nr + a.KT - 1) / a.KT;
+                        if (can_compact && tiles_now - tiles_new >= 2) {
+                            if (!compacted) {
+                                cperm = (int*)ws.get(W_PERM, (size_t)Kp * 8, &st_);
+                                if (st_ != ESL_OK) return st_;
+                                p2 = cperm + Kp;
+                                ESL_COUNT_LAUNCH();
+                                k_sw_iota<<<(Kp + 255) / 256, 256, 0, s>>>(Kp, cperm);
+                                add_perm(R, g.no, sizeof(TT));
+                                add_perm(R0, g.no, sizeof(TT));
+                                add_perm(PH, g.no, sizeof(TT));
+                                add_perm(V, g.no, sizeof(TT));
+                                add_perm(SH, g.no, sizeof(TT));
+                                add_perm(Tt, g.no, sizeof(TT));
+                                add_perm(D, g.no, sizeof(TT));
+                                add_perm(dS64, g.no, 8);
+                                add_perm(dS32, g.no, 4);
+                                add_perm(a.Qo, g.no, 8);
+                                add_perm(a.IQe, g.ne, 8);
+                                add_perm(a.rateT, 2 * n, 8);
+                                add_perm(scal, C_NSCAL, 8);
+                                add_perm(iscal, I_NISCAL, 4);
+                                compacted = true;
+                            }
+                            ESL_COUNT_LAUNCH();
+                            k_sw_perm_build<<<1, 1024, 0, s>>>(Kc, sc.i[I_FLAGS], cperm, p2);
+                            ESL_COUNT_LAUNCH();
+                            k_sw_row_perm<<<dim3(perm_blocks, npl), kPermWarps * 32, (size_t)kPermWarps * Kc * 8, s>>>(
+                                pl, Kp, Kc, p2, 0);
+                            ESL_CUDA(cudaGetLastError());
+                            Kc = tiles_new * a.KT;
+                            a.K = Kc;
+                            gei = row_grid(g.ne, Kc, a.KT, ctx->sm_count);
+                            goi = row_grid(g.no, Kc, a.KT, ctx->sm_count);
+                            gei2 = row_grid(g.ne, Kc, a.KT, ctx->sm_count, 2);
+                            goi2 = row_grid(g.no, Kc, a.KT, ctx->sm_count, 2);
+                            gp.reset();  // the poll-window graphs hold the old grid
+                            st.compactions++;
+                        }
                     }
+                }
+                if (compacted) {
+                    // every array back to the original system order
+                    ESL_COUNT_LAUNCH();
+                    k_sw_row_perm<<<dim3(perm_blocks, npl), kPermWarps * 32, (size_t)kPermWarps * Kp * 8, s>>>(
+                        pl, Kp, Kp, cperm, 1);
+                    ESL_CUDA(cudaGetLastError());
+                    a.K = K;
+                    gei = gei0;
+                    goi = goi0;
+                    gei2 = gei20;
+                    goi2 = goi20;
                 }
                 group_iters += it;
                 ESL_COUNT_LAUNCH();

@@ -143,7 +143,16 @@ def test_tensor_core_inference_matches_forward(esl, ctx, case):
     assert np.all(w[:, mask] == 0.0)
 
 
-def test_trained_warm_start_gain(esl, ctx, case, capsys):
+def test_trained_warm_start_effect(esl, ctx, case, capsys):
+    """What the trained warm start does to the mixed solve on held-out rate sets.
+
+    Measured, not a gain: the network learns (training loss at least halves, held-out
+    log-occupation error median ~0.4), the warm-started solve still converges and agrees
+    with the FP64 oracle, and its Krylov iteration count stays within 15% of the cold
+    start's either way (B200: cold 195-247, warm 200-259 on this case).  A start with a
+    ~40% relative error per state leaves a residual far above |b|, because the occupation
+    spans seven decades, so it cannot cut the iterations much (host replica: even a
+    1e-4-accurate start saves only 25-35%)."""
     rates = case["rates"]
     train, held = rates[:192], rates[192:]
     net = case["net"]
@@ -171,3 +180,4 @@ def test_trained_warm_start_gain(esl, ctx, case, capsys):
               f"{lerr.median().item():.3f} p90 {lerr.quantile(0.9).item():.3f}; Krylov iterations "
               f"cold {cold.report.iterations} warm {hot.report.iterations}")
     assert hot.report.converged == 1
+    assert abs(hot.report.iterations - cold.report.iterations) <= 0.15 * cold.report.iterations
