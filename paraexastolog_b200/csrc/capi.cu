@@ -122,7 +122,9 @@ int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out) {
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (cudaMallocHost(&c->h_flag, 64) != cudaSuccess || c->d_flag.alloc(8) != ESL_OK ||
         cudaEventCreateWithFlags(&c->poll_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->poll_ev[2], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->poll_ev[3], cudaEventDisableTiming) != cudaSuccess) {
         esl_ctx_destroy(c);
         return fail(ESL_ERR_NOMEM, "context allocation failed");
     }

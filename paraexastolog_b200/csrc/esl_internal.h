@@ -117,7 +117,7 @@ struct esl_ctx {
     esl::DevBuf<unsigned long long> d_flag;  // device counters (8 slots)
     void* work = nullptr;             // solver workspace (grow-only), freed with the context
     void* sweep_work = nullptr;       // level-sweep workspace (grow-only), freed with the context
-    cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // convergence polls of the level sweep
+    cudaEvent_t poll_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // convergence polls of the level sweep
     // level-sweep tiling of the last esl_net_autotune on this context (0 / -1: default),
     // used for networks that have no tuning of their own
     int tune_tile_mb = 0, tune_s2 = -1;

@@ -37,6 +37,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "esl_internal.h"
 
 namespace esl {
@@ -46,6 +48,12 @@ constexpr int kSwT = 256;            // threads per row kernel
 constexpr int kSwLocalMax = 512;     // largest SCC of a group solved CTA-locally
 constexpr int kSwLocalWarps = 16;    // most warps of a CTA-local solve
 constexpr int kSwPoll = 4;           // Krylov iterations launched between convergence polls
+// Poll windows in flight: the host reads the running count of window c - (depth - 1)
+// after queueing window c, so a late host leaves the GPU idle only after it has fallen
+// depth - 1 windows behind.  Windows queued past convergence cost little (tiles whose
+// systems have stopped exit at once).
+constexpr int kSwPollDepth = 3;
+static_assert(kSwPollDepth >= 2 && kSwPollDepth <= 4, "the context holds four poll events and count slots");
 constexpr double kSwAcceptRel = 1e-8;  // stagnating systems are accepted at this relative residual
 constexpr int kSwStall = 30;         // inner iterations without halving the residual before an inner solve stops
 // The same for the FP64 inner solves of grid-wide groups.  BiCGStab's residual there has
@@ -125,8 +133,9 @@ struct SwArgs {
 };
 
 // A tile is KT systems of one row handled by TR = KT / S threads, S systems per thread:
-// thread `lane` of the row owns systems k, k + TR, ..., k + (S - 1) TR.  TR >= 32, so the
-// 32 lanes of a warp always share one row.
+// thread `lane` of the row owns the adjacent systems k = lane * S, ..., k + S - 1 of the
+// tile, so that its S values of a row are one vector load.  TR >= 32, so the 32 lanes of
+// a warp always share one row.
 struct Tile {
     int lane, rsub, RB, KT, TR, k;
 };
@@ -139,8 +148,25 @@ __device__ __forceinline__ Tile tile_of(int KT) {
     t.RB = blockDim.x / t.TR;
     t.lane = threadIdx.x % t.TR;
     t.rsub = threadIdx.x / t.TR;
-    t.k = blockIdx.y * KT + t.lane;
+    t.k = blockIdx.y * KT + t.lane * S;
     return t;
+}
+
+// S adjacent values of a row (8- or 4-byte elements), one vector load when S == 2
+template <int S, class TX>
+__device__ __forceinline__ void load_s(const TX* __restrict__ p, TX (&v)[S]) {
+    if constexpr (S == 2 && sizeof(TX) == 8) {
+        const double2 w = *reinterpret_cast<const double2*>(p);
+        v[0] = (TX)w.x;
+        v[1] = (TX)w.y;
+    } else if constexpr (S == 2 && sizeof(TX) == 4) {
+        const float2 w = *reinterpret_cast<const float2*>(p);
+        v[0] = (TX)w.x;
+        v[1] = (TX)w.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < S; q++) v[q] = p[q];
+    }
 }
 
 template <class T>
@@ -162,9 +188,9 @@ __device__ __forceinline__ void sw_qs(const T* s, uint32_t v, uint32_t f, const 
     while (f) {
         const int i = __ffs(f) - 1;
         f &= f - 1;
-        const T* r = s + (2 * i + ((v >> i) & 1u)) * t.KT + t.lane;
+        const T* r = s + (2 * i + ((v >> i) & 1u)) * t.KT + t.lane * S;
 #pragma unroll
-        for (int j = 0; j < S; j++) q[j] += r[j * t.TR];
+        for (int j = 0; j < S; j++) q[j] += r[j];
     }
 }
 
@@ -196,39 +222,64 @@ __device__ __forceinline__ bool sw_skip(const SwArgs& a, int k) {
 // at a time.  Every lane of the warp must call it; systems with act[j] == false load
 // nothing.
 template <int S, class TC, class TX>
-__device__ __forceinline__ void sw_gathers(const TC* s, const Tile& t, int Kp, const uint32_t* __restrict__ ent,
-                                           uint32_t p0, int cnt, const TX* __restrict__ X, uint32_t base,
-                                           const bool (&act)[S], TC (&acc)[S]) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t mine = lane < cnt ? __ldg(ent + p0 + lane) : 0u;
+__device__ __forceinline__ void sw_gathers_m(const TC* s, const Tile& t, int Kp, uint32_t mine, int cnt,
+                                             const TX* __restrict__ X, uint32_t base, const bool (&act)[S],
+                                             TC (&acc)[S]) {
     const TX* Xk = X + t.k;
-    const TC* sk = s + t.lane;
+    const TC* sk = s + t.lane * S;
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < S; q++) any |= act[q];
+    // a thread loads its S adjacent values of a row together (inactive ones are read and
+    // then ignored: they share the load)
     int j = 0;
     for (; j + 4 <= cnt; j += 4) {
         uint32_t e[4];
-        TC x[4][S];
+        TX x[4][S];
 #pragma unroll
         for (int u = 0; u < 4; u++) e[u] = __shfl_sync(0xffffffffu, mine, j + u);
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const TX* row = Xk + (size_t)(ent_slot(e[u]) - base) * Kp;
+            if (any) {
+                load_s<S, TX>(row, x[u]);
+            } else {
 #pragma unroll
-            for (int q = 0; q < S; q++) x[u][q] = act[q] ? (TC)row[q * t.TR] : (TC)0;
+                for (int q = 0; q < S; q++) x[u][q] = (TX)0;
+            }
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const TC* r = sk + ent_rate(e[u]) * t.KT;
+            TC r[S];
+            load_s<S, TC>(sk + ent_rate(e[u]) * t.KT, r);
 #pragma unroll
-            for (int q = 0; q < S; q++) acc[q] += r[q * t.TR] * x[u][q];
+            for (int q = 0; q < S; q++) acc[q] += r[q] * (act[q] ? (TC)x[u][q] : (TC)0);
         }
     }
     for (; j < cnt; j++) {
         const uint32_t e = __shfl_sync(0xffffffffu, mine, j);
         const TX* row = Xk + (size_t)(ent_slot(e) - base) * Kp;
-        const TC* r = sk + ent_rate(e) * t.KT;
+        TX x[S];
+        if (any) {
+            load_s<S, TX>(row, x);
+        } else {
 #pragma unroll
-        for (int q = 0; q < S; q++) acc[q] += r[q * t.TR] * (act[q] ? (TC)row[q * t.TR] : (TC)0);
+            for (int q = 0; q < S; q++) x[q] = (TX)0;
+        }
+        TC r[S];
+        load_s<S, TC>(sk + ent_rate(e) * t.KT, r);
+#pragma unroll
+        for (int q = 0; q < S; q++) acc[q] += r[q] * (act[q] ? (TC)x[q] : (TC)0);
     }
+}
+
+template <int S, class TC, class TX>
+__device__ __forceinline__ void sw_gathers(const TC* s, const Tile& t, int Kp, const uint32_t* __restrict__ ent,
+                                           uint32_t p0, int cnt, const TX* __restrict__ X, uint32_t base,
+                                           const bool (&act)[S], TC (&acc)[S]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t mine = lane < cnt ? __ldg(ent + p0 + lane) : 0u;
+    sw_gathers_m<S, TC, TX>(s, t, Kp, mine, cnt, X, base, act, acc);
 }
 
 template <class TC, class TX>
@@ -256,7 +307,7 @@ __device__ __forceinline__ void sw_reduce(const double (&v)[NV][S], double* cons
         for (int j = 0; j < NV; j++)
 #pragma unroll
             for (int q = 0; q < S; q++) {
-                const int k = t.k + q * t.TR;
+                const int k = t.k + q;
                 if (k >= K) continue;
                 double acc = 0.0;
                 for (int r = 0; r < t.RB; r++) acc += red[(j * S + q) * kSwT + r * t.TR + t.lane];
@@ -353,7 +404,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
     double wsum[S];
 #pragma unroll
     for (int q = 0; q < S; q++) {
-        act[q] = !sw_skip(a, t.k + q * t.TR);
+        act[q] = !sw_skip(a, t.k + q);
         any |= act[q];
         wsum[q] = 0.0;
     }
@@ -367,14 +418,14 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
         const size_t idx = (size_t)r * a.Kp + t.k;
         TC acc[S];
 #pragma unroll
-        for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q * t.TR] : (TC)0;
+        for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q] : (TC)0;
         if (X) sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, X, obase, act, acc);
         if (sizeof(TC) == 8 && a.IQe) {
 #pragma unroll
             for (int q = 0; q < S; q++)
                 if (act[q]) {
-                    const TW w = (TW)(acc[q] * (TC)__ldcs(a.IQe + idx + q * t.TR));
-                    W[idx + q * t.TR] = w;
+                    const TW w = (TW)(acc[q] * (TC)__ldcs(a.IQe + idx + q));
+                    W[idx + q] = w;
                     if (DEFL) wsum[q] += (double)w;
                 }
         } else {
@@ -384,7 +435,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
             for (int q = 0; q < S; q++)
                 if (act[q]) {
                     const TW w = (TW)(acc[q] / qv[q]);
-                    W[idx + q * t.TR] = w;
+                    W[idx + q] = w;
                     if (DEFL) wsum[q] += (double)w;
                 }
         }
@@ -425,7 +476,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
 #pragma unroll
     for (int q = 0; q < S; q++) {
         d0[q] = d1[q] = d2[q] = dg[q] = 0.0;
-        const int k = t.k + q * t.TR;
+        const int k = t.k + q;
         act[q] = !((MODE >= 2) ? sw_skip(a, k) : (k >= a.K));
         any |= act[q];
     }
@@ -441,7 +492,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
             if (MODE != 0) {
                 if (sizeof(T) == 8 && a.Qo) {
 #pragma unroll
-                    for (int q = 0; q < S; q++) qv[q] = act[q] ? (T)__ldcs(a.Qo + idx + q * t.TR) : (T)0;
+                    for (int q = 0; q < S; q++) qv[q] = act[q] ? (T)__ldcs(a.Qo + idx + q) : (T)0;
                 } else {
                     sw_qs<S>(s_rate, d.x, d.y, t, qv);
                 }
@@ -449,7 +500,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
 #pragma unroll
             for (int q = 0; q < S; q++) {
                 if (!act[q]) continue;
-                const size_t i = idx + q * t.TR;
+                const size_t i = idx + q;
                 if (MODE == 0) {
                     const double y = B[i] + (double)flow[q];
                     Y[i] = (T)y;
@@ -1627,15 +1678,15 @@ dim3 row_grid(uint32_t rows, int Kp, int KT, int sm_count, int S = 1) {
     return dim3((unsigned)want, ty);
 }
 
-// the two graphs (one per poll-slot parity) of a Krylov solve, released on scope exit
+// the graphs (one per poll slot) of a Krylov solve, released on scope exit
 struct GraphPair {
-    cudaGraph_t graph[2] = {nullptr, nullptr};
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraph_t graph[kSwPollDepth] = {};
+    cudaGraphExec_t exec[kSwPollDepth] = {};
     GraphPair() = default;
     GraphPair(const GraphPair&) = delete;
     GraphPair& operator=(const GraphPair&) = delete;
     void reset() {
-        for (int p = 0; p < 2; p++) {
+        for (int p = 0; p < kSwPollDepth; p++) {
             if (exec[p]) cudaGraphExecDestroy(exec[p]);
             if (graph[p]) cudaGraphDestroy(graph[p]);
             exec[p] = nullptr;
@@ -1903,6 +1954,18 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
             }
             continue;
         }
+        // An NVTX range names the grid solve of the largest level group, so that a
+        // profiler can select that group's launches (`ncu --nvtx --nvtx-include
+        // "esl_largest_level_group/"`); without a profiler attached it costs nothing.
+        struct NvtxRange {
+            bool on;
+            explicit NvtxRange(bool b) : on(b) {
+                if (on) nvtxRangePushA("esl_largest_level_group");
+            }
+            ~NvtxRange() {
+                if (on) nvtxRangePop();
+            }
+        } nvtx_range(!term && g.ne + g.no == P->max_rows);
         auto true_residual = [&]() -> int {
             a.flags = nullptr;
             a.KT = gKT64;
@@ -2091,7 +2154,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                 cudaGraphExec_t* gexec = gp.exec;
                 int it = 0, chunk = 0;
                 for (; it < max_iters; it += kSwPoll, chunk++) {
-                    const int par = chunk & 1;
+                    const int par = chunk % kSwPollDepth;  // the window's running-count slot
                     if (chunk == 0 || !capturable) {
                         ESL_TRY(launch_chunk(par, ctx->prof && chunk == 0));
                     } else if (!gexec[par]) {
@@ -2116,17 +2179,18 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                     }
                 poll:
                     ESL_CUDA(cudaMemcpyAsync(h_cnt + 1 + par, d_cnt + 1 + par, 4, cudaMemcpyDeviceToHost, s));
-                    ESL_CUDA(cudaEventRecord(ctx->poll_ev[chunk & 1], s));
-                    if (chunk >= 1) {
-                        ESL_CUDA(cudaEventSynchronize(ctx->poll_ev[(chunk - 1) & 1]));
-                        const int nr = h_cnt[1 + ((chunk - 1) & 1)];
+                    ESL_CUDA(cudaEventRecord(ctx->poll_ev[par], s));
+                    if (chunk >= kSwPollDepth - 1) {
+                        const int old_slot = (chunk - (kSwPollDepth - 1)) % kSwPollDepth;
+                        ESL_CUDA(cudaEventSynchronize(ctx->poll_ev[old_slot]));
+                        const int nr = h_cnt[1 + old_slot];
                         if (nr == 0) {
                             it += kSwPoll;
                             break;
                         }
-                        // The count is that of the window before the one in flight, an upper
+                        // The count is that of a window before the ones in flight, an upper
                         // bound of the systems still running when the compaction (queued
-                        // behind that window) runs.
+                        // behind them) runs.
                         const int tiles_now = Kc / a.KT, tiles_new = (nr + a.KT - 1) / a.KT;
                         if (can_compact && tiles_now - tiles_new >= 2) {
                             if (!compacted) {
