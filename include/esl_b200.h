@@ -121,6 +121,11 @@ int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char*
 int esl_table_nnz(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* nnz);
 int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32_t* d_indptr,
                     int32_t* d_rows, int32_t* d_cols);
+/* The same CSC with 64-bit column pointers (d_indptr[N+1] int64), for tables of 2^31 or
+ * more edges, which the reference's index_t = int (cuda/src/types.h:6) cannot address:
+ * networks of up to ESL_MAX_NODES nodes (n = 28: about 3.8e9 edges, 17 GB). */
+int esl_table_build64(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* d_indptr,
+                      int32_t* d_rows, int32_t* d_cols);
 /* per-state flip masks: bit i of d_out[s] = edge s -> s^(1<<i); of d_in[s] = edge s^(1<<i) -> s */
 int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in);
 
@@ -274,6 +279,11 @@ int esl_ctx_profile_records(esl_ctx* ctx, int cap, double* ms, double* bytes, in
 int esl_ctx_profile_entry(esl_ctx* ctx, int i, const char** name, double* ms, double* bytes);
 /* number of kernels this library has launched in this process (no counterpart in the reference) */
 int esl_launch_count(uint64_t* count);
+/* The library keeps the device blocks it releases (up to 8 GiB per device) and hands them
+ * out again, because cudaFree / cudaMalloc of a network's symbolic buffers cost up to
+ * 0.8 s per build on the B200.  This returns every cached block to the driver (no
+ * counterpart in the reference). */
+int esl_trim_cache(void);
 
 #ifdef __cplusplus
 }

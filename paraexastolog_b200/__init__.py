@@ -94,6 +94,8 @@ def lib():
     L.esl_table_nnz.argtypes = [vp, vp, vp, P(C.c_int64)]
     L.esl_table_build.argtypes = [vp, vp, vp, vp, vp, vp]
     L.esl_flip_masks.argtypes = [vp, vp, vp, vp, vp]
+    L.esl_table_build64.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.esl_trim_cache.argtypes = []
     L.esl_table_build_static.argtypes = [vp, vp, vp, vp, vp, vp, C.c_int64, P(C.c_int64)]
     L.esl_net_build.argtypes = [vp, vp, vp, P(vp)]
     L.esl_net_from_csc.argtypes = [vp, C.c_int, vp, vp, P(vp)]
@@ -122,6 +124,11 @@ def lib():
     L.esl_mlp_predict.argtypes = [vp, C.c_int, vp, vp]
     _lib = L
     return L
+
+
+def trim_cache():
+    """Return the library's cached device blocks to the driver."""
+    check(lib().esl_trim_cache())
 
 
 def launch_count() -> int:
@@ -298,6 +305,21 @@ def table(ctx: Context, model: Model, rates: np.ndarray, with_cols: bool = True)
     rows = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
     cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev) if with_cols else None
     check(lib().esl_table_build(ctx._h, model._h, _ptr(rates), _ptr(indptr), _ptr(rows), _ptr(cols)))
+    return indptr, rows[: nnz.value], (cols[: nnz.value] if with_cols else None)
+
+
+def table64(ctx: Context, model: Model, rates: np.ndarray, with_cols: bool = False):
+    """CSC transition table with int64 column pointers (tables of >= 2^31 edges):
+    (indptr int64, rows int32, cols int32 or None) device tensors."""
+    torch = _torch()
+    rates = np.ascontiguousarray(rates, np.float64)
+    nnz = C.c_int64()
+    check(lib().esl_table_nnz(ctx._h, model._h, _ptr(rates), C.byref(nnz)))
+    dev = f"cuda:{ctx.device}"
+    indptr = torch.empty((1 << model.n) + 1, dtype=torch.int64, device=dev)
+    rows = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+    cols = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev) if with_cols else None
+    check(lib().esl_table_build64(ctx._h, model._h, _ptr(rates), _ptr(indptr), _ptr(rows), _ptr(cols)))
     return indptr, rows[: nnz.value], (cols[: nnz.value] if with_cols else None)
 
 

@@ -3,6 +3,9 @@
 
 #include <atomic>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 #include <cstring>
 #include <fstream>
 #include <random>
@@ -17,6 +20,121 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// ---- device memory cache (declared in esl_internal.h) ----------------------------------
+namespace {
+struct Block {
+    size_t bytes;
+    int dev;
+};
+std::mutex g_pool_mu;
+std::unordered_map<void*, Block> g_pool_live;               // handed out
+std::multimap<std::pair<int, size_t>, void*> g_pool_free;    // (device, size class) -> cached block
+std::unordered_map<int, size_t> g_pool_cached;              // cached bytes per device
+// cached bytes a device may keep; beyond it the largest cached blocks are freed
+constexpr size_t kPoolCap = (size_t)8 << 30;
+
+// size classes: powers of two up to 1 MiB, then multiples of 2 MiB
+size_t size_class(size_t b) {
+    if (b <= 256) return 256;
+    if (b <= ((size_t)1 << 20)) {
+        size_t c = 256;
+        while (c < b) c <<= 1;
+        return c;
+    }
+    const size_t g = (size_t)2 << 20;
+    return (b + g - 1) / g * g;
+}
+
+// frees every cached block of device `dev` (the caller holds the lock)
+void pool_trim(int dev) {
+    for (auto it = g_pool_free.begin(); it != g_pool_free.end();) {
+        if (it->first.first == dev) {
+            cudaFree(it->second);
+            it = g_pool_free.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    g_pool_cached[dev] = 0;
+}
+}  // namespace
+
+void* dev_alloc(size_t bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const size_t c = size_class(bytes);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pool_free.find({dev, c});
+    if (it != g_pool_free.end()) {
+        void* p = it->second;
+        g_pool_free.erase(it);
+        g_pool_cached[dev] -= c;
+        g_pool_live[p] = Block{c, dev};
+        return p;
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, c) != cudaSuccess) {
+        cudaGetLastError();  // clear the allocation error
+        pool_trim(dev);
+        p = nullptr;
+        if (cudaMalloc(&p, c) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    g_pool_live[p] = Block{c, dev};
+    return p;
+}
+
+thread_local cudaStream_t t_api_stream = nullptr;
+thread_local bool t_released_synced = false;
+
+void dev_free(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pool_live.find(p);
+    if (it == g_pool_live.end()) return;
+    const Block b = it->second;
+    g_pool_live.erase(it);
+    // as cudaFree: no work on the block may still run when it is handed out again
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != b.dev) cudaSetDevice(b.dev);
+    if (!t_released_synced) {
+        if (t_api_stream)
+            cudaStreamSynchronize(t_api_stream);
+        else
+            cudaDeviceSynchronize();
+    }
+    g_pool_free.insert({{b.dev, b.bytes}, p});
+    size_t& cached = g_pool_cached[b.dev];
+    cached += b.bytes;
+    while (cached > kPoolCap) {
+        // the device's largest cached block
+        auto last = g_pool_free.upper_bound({b.dev, SIZE_MAX});
+        if (last == g_pool_free.begin()) break;
+        --last;
+        if (last->first.first != b.dev) break;
+        cudaFree(last->second);
+        cached -= last->first.second;
+        g_pool_free.erase(last);
+    }
+    if (cur != b.dev) cudaSetDevice(cur);
+}
+
+void dev_trim_all() {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto& kv : g_pool_free) {
+        cudaSetDevice(kv.first.first);
+        cudaFree(kv.second);
+    }
+    g_pool_free.clear();
+    g_pool_cached.clear();
+    cudaSetDevice(cur);
+}
 
 void set_error(const std::string& msg) { g_error = msg; }
 int fail(int code, const std::string& msg) {
@@ -95,6 +213,11 @@ extern "C" {
 const char* esl_last_error(void) { return g_error.c_str(); }
 int esl_version(void) { return 100; }
 
+int esl_trim_cache(void) {
+    dev_trim_all();
+    return ESL_OK;
+}
+
 int esl_launch_count(uint64_t* count) {
     if (!count) return fail(ESL_ERR_INVALID, "NULL argument");
     *count = g_launches.load();
@@ -133,6 +256,7 @@ int esl_ctx_create(int device, void* cuda_stream, esl_ctx** out) {
 }
 
 int esl_ctx_destroy(esl_ctx* c) {
+    StreamScope stream_scope_(c);
     if (!c) return ESL_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->work) free_workspace(c->work);
@@ -207,10 +331,12 @@ int esl_ctx_profile_entry(esl_ctx* c, int i, const char** name, double* ms, doub
 
 int esl_net_autotune(esl_ctx* c, esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                      const esl_solve_opts* opts, int* tile_mb, int* two_per_thread, double* ms_out) {
+    StreamScope stream_scope_(c);
     if (!c || !net || !d_rates || !d_x0 || B < 1 || R < 1) return fail(ESL_ERR_INVALID, "bad argument");
     const size_t N = (size_t)net->N;
-    double *xi = nullptr;
-    if (cudaMalloc(&xi, (size_t)B * R * N * 8) != cudaSuccess) return fail(ESL_ERR_NOMEM, "autotune buffer");
+    DevBuf<double> xbuf;
+    ESL_TRY(xbuf.alloc((size_t)B * R * N));
+    double* xi = xbuf.get();
     struct Cand {
         int mb, s2;
     };
@@ -240,7 +366,6 @@ int esl_net_autotune(esl_ctx* c, esl_net* net, int B, const double* d_rates, int
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaFree(xi);
     if (best < 0) {
         net->tune_tile_mb = 0;
         net->tune_s2 = -1;
@@ -375,6 +500,7 @@ int esl_rates_normal(const esl_model* m, double mean, double stddev, uint64_t se
 
 int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char* const* fixed_names,
                       const int* fixed_values, double fixed_probability, double* d_x0) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !d_x0 || (n_fixed > 0 && (!fixed_names || !fixed_values)))
         return fail(ESL_ERR_INVALID, "NULL argument");
     const int n = m->m.n();
@@ -407,6 +533,7 @@ int esl_initial_state(esl_ctx* ctx, const esl_model* m, int n_fixed, const char*
 }
 
 int esl_table_nnz(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* nnz) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !nnz) return fail(ESL_ERR_INVALID, "NULL argument");
     DevBuf<uint32_t> F, G, counts;
     ESL_TRY(table_pass(ctx, m->m, rates, F, G, counts, *nnz, false));
@@ -415,6 +542,7 @@ int esl_table_nnz(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t
 
 int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32_t* d_indptr, int32_t* d_rows,
                     int32_t* d_cols) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !d_indptr || !d_rows) return fail(ESL_ERR_INVALID, "NULL argument");
     DevBuf<uint32_t> F, G, counts;
     int64_t nnz = 0;
@@ -439,7 +567,37 @@ int esl_table_build(esl_ctx* ctx, const esl_model* m, const double* rates, int32
     return ESL_OK;
 }
 
+int esl_table_build64(esl_ctx* ctx, const esl_model* m, const double* rates, int64_t* d_indptr, int32_t* d_rows,
+                      int32_t* d_cols) {
+    StreamScope stream_scope_(ctx);
+    if (!ctx || !m || !d_indptr || !d_rows) return fail(ESL_ERR_INVALID, "NULL argument");
+    DevBuf<uint32_t> F, G, counts;
+    int64_t nnz = 0;
+    ESL_TRY(table_pass(ctx, m->m, rates, F, G, counts, nnz, false));
+    const int64_t blocks = flip_mask_blocks(m->m.n());
+    DevBuf<uint64_t> offs;
+    ESL_TRY(offs.alloc(blocks));
+    // 64-bit running sum of the 32-bit block counts (the initial value sets the sum's type)
+    size_t tmp = 0;
+    ESL_CUDA(cub::DeviceScan::ExclusiveScan(nullptr, tmp, counts.get(), offs.get(), cub::Sum(), (uint64_t)0,
+                                            (int)blocks, ctx->stream));
+    DevBuf<uint8_t> tbuf;
+    ESL_TRY(tbuf.alloc(tmp));
+    ESL_CUDA(cub::DeviceScan::ExclusiveScan(tbuf.get(), tmp, counts.get(), offs.get(), cub::Sum(), (uint64_t)0,
+                                            (int)blocks, ctx->stream));
+    {
+        // algorithmic bytes: the out-masks read (4 B per state), indptr written (8 B per
+        // state), destinations (and sources) written (4 B per edge each)
+        const double N = (double)(1ull << m->m.n());
+        ProfScope ps(ctx, "k_emit_csc64", 12.0 * N + 8.0 + (d_cols ? 8.0 : 4.0) * (double)nnz);
+        ESL_TRY(launch_emit_csc64(m->m.n(), F.get(), offs.get(), d_indptr, d_rows, d_cols, nnz, ctx->stream));
+    }
+    ESL_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ESL_OK;
+}
+
 int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32_t* d_out, uint32_t* d_in) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !d_out) return fail(ESL_ERR_INVALID, "NULL argument");
     ESL_TRY(check_rates(m->m, rates));
     DevModelBufs mb;
@@ -451,6 +609,7 @@ int esl_flip_masks(esl_ctx* ctx, const esl_model* m, const double* rates, uint32
 }
 
 int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net** out) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !out) return fail(ESL_ERR_INVALID, "NULL argument");
     *out = nullptr;
     ESL_TRY(check_rates(m->m, rates));
@@ -474,6 +633,7 @@ int esl_net_build(esl_ctx* ctx, const esl_model* m, const double* rates, esl_net
 }
 
 int esl_net_from_csc(esl_ctx* ctx, int n_nodes, const int32_t* d_indptr, const int32_t* d_rows, esl_net** out) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !d_indptr || !d_rows || !out) return fail(ESL_ERR_INVALID, "NULL argument");
     if (n_nodes < 1 || n_nodes > ESL_MAX_NODES) return fail(ESL_ERR_INVALID, "node count out of range");
     *out = nullptr;
@@ -503,7 +663,13 @@ int esl_net_from_csc(esl_ctx* ctx, int n_nodes, const int32_t* d_indptr, const i
 }
 
 int esl_net_free(esl_net* net) {
+    if (!net) return ESL_OK;
+    // a net's buffers may have been read on any context's stream: one device-wide wait,
+    // then its blocks go back to the cache without further waits
+    cudaDeviceSynchronize();
+    t_released_synced = true;
     delete net;
+    t_released_synced = false;
     return ESL_OK;
 }
 
@@ -518,6 +684,7 @@ int esl_net_info(const esl_net* net, int* n_nodes, int* n_sccs, int* n_terminals
 
 int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* d_offsets, int32_t* d_levels,
                    int32_t* d_labels) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !net) return fail(ESL_ERR_INVALID, "NULL argument");
     cudaStream_t s = ctx->stream;
     if (d_order) ESL_CUDA(cudaMemcpyAsync(d_order, net->order.get(), net->N * 4, cudaMemcpyDeviceToDevice, s));
@@ -560,6 +727,7 @@ static int check_batch_rates(esl_ctx* ctx, const esl_net* net, int B, const doub
 
 int esl_solve(esl_ctx* ctx, const esl_net* net, const double* d_rates, const double* d_x0, double* d_x_inf,
               double* d_marginals, double* d_R, double* d_L, const esl_solve_opts* opts, esl_report* report) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !net || !d_rates || !d_x0) return fail(ESL_ERR_INVALID, "NULL argument");
     ESL_TRY(check_batch_rates(ctx, net, 1, d_rates));
     return solve_batch(ctx, net, 1, d_rates, 1, d_x0, d_x_inf, d_marginals, d_R, d_L, opts, report);
@@ -567,6 +735,7 @@ int esl_solve(esl_ctx* ctx, const esl_net* net, const double* d_rates, const dou
 
 int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                     double* d_x_inf, double* d_marginals, const esl_solve_opts* opts, esl_report* report) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !net || !d_rates || !d_x0) return fail(ESL_ERR_INVALID, "NULL argument");
     if (B < 1 || R < 1 || (int64_t)B * R > 65535) return fail(ESL_ERR_INVALID, "B*R must be in [1, 65535]");
     ESL_TRY(check_batch_rates(ctx, net, B, d_rates));
@@ -575,6 +744,7 @@ int esl_solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rat
 
 int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates, int R, const double* x0,
                    double* x_inf, double* marginals, const esl_solve_opts* opts, esl_report* report) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !m || !rates || !x0 || !x_inf) return fail(ESL_ERR_INVALID, "NULL argument");
     if (B < 1 || R < 1) return fail(ESL_ERR_INVALID, "B and R must be positive");
     const int n = m->m.n();

@@ -47,7 +47,26 @@ struct Model {
 
 int parse_bnet(const std::string& text, Model& out);
 
-// ---- device buffers -----------------------------------------------------------
+// ---- device memory cache --------------------------------------------------------
+// Every device buffer of the library comes from a process-wide cache per device.  A
+// released block stays mapped and is handed out again for a request of its size class:
+// cudaFree / cudaMalloc of the ~25 buffers that a network's symbolic data and its
+// temporaries hold took up to 0.8 s per build-and-free on the B200 (driver-side
+// unmapping), against microseconds for the cache.  A release synchronises the device
+// first, as cudaFree does, so a block is never handed out while work on it may still
+// run (on the calling API's stream, else on the device).  A device keeps at most 8 GiB of
+// cached blocks (the largest go first); when cudaMalloc fails the device's cached blocks
+// are freed and the request is retried once.
+void* dev_alloc(size_t bytes);  // nullptr on failure
+void dev_free(void* p);
+void dev_trim_all();            // frees every cached block of every device
+// The stream of the API call running on this thread, or nullptr: a released block waits
+// for that stream only.  A device-wide synchronisation could invalidate a CUDA-graph
+// capture that another thread (another context of esl_solve_many) has in progress.
+extern thread_local cudaStream_t t_api_stream;
+// set while a caller that has already synchronised the device releases its blocks
+extern thread_local bool t_released_synced;
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
@@ -57,18 +76,15 @@ struct DevBuf {
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }
     int alloc(size_t count) {
         release();
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail(ESL_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        }
+        p = static_cast<T*>(dev_alloc(count * sizeof(T)));
+        if (!p) return fail(ESL_ERR_NOMEM, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
         n = count;
         return ESL_OK;
     }
@@ -82,11 +98,11 @@ struct Workspace {
         if ((int)bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
         auto& b = bufs[slot];
         if (b.second < bytes) {
-            if (b.first) cudaFree(b.first);
+            if (b.first) dev_free(b.first);
             b.first = nullptr;
             b.second = 0;
-            if (cudaMalloc(&b.first, bytes) != cudaSuccess) {
-                b.first = nullptr;
+            b.first = dev_alloc(bytes);
+            if (!b.first) {
                 *status = fail(ESL_ERR_NOMEM, "workspace allocation of " + std::to_string(bytes) + " bytes failed");
                 return nullptr;
             }
@@ -101,7 +117,7 @@ struct Workspace {
     }
     ~Workspace() {
         for (auto& b : bufs)
-            if (b.first) cudaFree(b.first);
+            if (b.first) dev_free(b.first);
     }
 };
 
@@ -182,6 +198,17 @@ struct esl_net {
 
 namespace esl {
 
+// Sets the stream of the API call on this thread for its lifetime (see t_api_stream).
+struct StreamScope {
+    cudaStream_t prev;
+    explicit StreamScope(const esl_ctx* c) : prev(t_api_stream) {
+        if (c) t_api_stream = c->stream;
+    }
+    ~StreamScope() { t_api_stream = prev; }
+    StreamScope(const StreamScope&) = delete;
+    StreamScope& operator=(const StreamScope&) = delete;
+};
+
 // Measurement hook: when profiling is on, CUDA events on the context's stream bracket
 // the launches made while the scope lives; the record carries the kernel class and
 // the algorithmic bytes of those launches.
@@ -248,6 +275,9 @@ int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* bl
 int64_t flip_mask_blocks(int n);
 int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
                     int32_t* cols, int64_t nnz, cudaStream_t s);
+// the same with 64-bit block offsets and column pointers (tables of >= 2^31 edges)
+int launch_emit_csc64(int n, const uint32_t* F, const uint64_t* block_offsets_excl, int64_t* indptr, int32_t* rows,
+                      int32_t* cols, int64_t nnz, cudaStream_t s);
 int masks_from_csc(int n, const int32_t* indptr, const int32_t* rows, uint32_t* F, uint32_t* G,
                    unsigned long long* d_bad, cudaStream_t s);
 

@@ -554,6 +554,7 @@ int build_reach(esl_mlp* m) {
 extern "C" {
 
 int esl_mlp_create(esl_ctx* ctx, const esl_net* net, uint64_t seed, esl_mlp** out) {
+    StreamScope stream_scope_(ctx);
     if (!ctx || !net || !out) return fail(ESL_ERR_INVALID, "NULL argument");
     if (net->n > kBits) return fail(ESL_ERR_TOO_LARGE, "the learned warm start takes networks of at most 20 nodes");
     auto* m = new esl_mlp();
@@ -603,6 +604,7 @@ int esl_mlp_create(esl_ctx* ctx, const esl_net* net, uint64_t seed, esl_mlp** ou
 }
 
 int esl_mlp_free(esl_mlp* m) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (m) {
         cudaStreamSynchronize(m->ctx->stream);
         delete m;
@@ -611,6 +613,7 @@ int esl_mlp_free(esl_mlp* m) {
 }
 
 int esl_mlp_info(const esl_mlp* m, int* n_targets, float* mu, float* sigma) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m) return fail(ESL_ERR_INVALID, "mlp is NULL");
     if (n_targets) *n_targets = m->nt;
     if (mu) *mu = m->mu;
@@ -619,6 +622,7 @@ int esl_mlp_info(const esl_mlp* m, int* n_targets, float* mu, float* sigma) {
 }
 
 int esl_mlp_targets(const esl_mlp* m, uint32_t* d_states) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || !d_states) return fail(ESL_ERR_INVALID, "NULL argument");
     if (m->nt > 0)
         ESL_CUDA(cudaMemcpyAsync(d_states, m->targets.get(), (size_t)m->nt * 4, cudaMemcpyDeviceToDevice,
@@ -627,12 +631,14 @@ int esl_mlp_targets(const esl_mlp* m, uint32_t* d_states) {
 }
 
 int esl_mlp_reach(const esl_mlp* m, uint32_t* d_reach) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || !d_reach) return fail(ESL_ERR_INVALID, "NULL argument");
     ESL_CUDA(cudaMemcpyAsync(d_reach, m->reach.get(), (size_t)m->N * 4, cudaMemcpyDeviceToDevice, m->ctx->stream));
     return ESL_OK;
 }
 
 int esl_mlp_get_params(const esl_mlp* m, float* params) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || !params) return fail(ESL_ERR_INVALID, "NULL argument");
     ESL_CUDA(cudaMemcpyAsync(params, m->P.get(), kParams * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
     ESL_CUDA(cudaStreamSynchronize(m->ctx->stream));
@@ -640,6 +646,7 @@ int esl_mlp_get_params(const esl_mlp* m, float* params) {
 }
 
 int esl_mlp_set_params(esl_mlp* m, const float* params, float mu, float sigma) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || !params) return fail(ESL_ERR_INVALID, "NULL argument");
     if (!(sigma > 0.0f) || !std::isfinite(mu)) return fail(ESL_ERR_INVALID, "sigma must be > 0 and mu finite");
     ESL_CUDA(cudaMemcpyAsync(m->P.get(), params, kParams * 4, cudaMemcpyHostToDevice, m->ctx->stream));
@@ -653,6 +660,7 @@ int esl_mlp_set_params(esl_mlp* m, const float* params, float mu, float sigma) {
 
 int esl_mlp_features(esl_mlp* m, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
                      float* d_x) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || S < 0 || (S > 0 && (!d_rates || !d_k || !d_state || !d_x))) return fail(ESL_ERR_INVALID, "bad argument");
     if (S == 0) return ESL_OK;
     ESL_COUNT_LAUNCH();
@@ -664,6 +672,7 @@ int esl_mlp_features(esl_mlp* m, int S, const double* d_rates, const int32_t* d_
 
 int esl_mlp_loss_grad(esl_mlp* m, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
                       const float* d_target, float* loss, float* grad) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || S <= 0 || !d_rates || !d_k || !d_state || !d_target || !loss)
         return fail(ESL_ERR_INVALID, "bad argument");
     cudaStream_t s = m->ctx->stream;
@@ -683,6 +692,7 @@ int esl_mlp_loss_grad(esl_mlp* m, int S, const double* d_rates, const int32_t* d
 
 int esl_mlp_train(esl_mlp* m, int B, const double* d_rates, const double* d_occupation, int steps, int batch, float lr,
                   float* final_loss) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || B <= 0 || !d_rates || !d_occupation || steps < 0 || batch <= 0 || !(lr > 0.0f))
         return fail(ESL_ERR_INVALID, "bad argument");
     if (m->nt == 0) return fail(ESL_ERR_INVALID, "the network has no state that takes a warm start");
@@ -731,6 +741,7 @@ int esl_mlp_train(esl_mlp* m, int B, const double* d_rates, const double* d_occu
 }
 
 int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || B <= 0 || !d_rates || !d_warm) return fail(ESL_ERR_INVALID, "bad argument");
     cudaStream_t s = m->ctx->stream;
     ESL_CUDA(cudaMemsetAsync(d_warm, 0, (size_t)B * m->N * 8, s));
@@ -763,6 +774,7 @@ int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
 // written as predicted occupations; used to check the tensor-core inference
 int esl_mlp_forward(esl_mlp* m, int S, const double* d_rates, const int32_t* d_k, const int32_t* d_state,
                     float* d_y) {
+    StreamScope stream_scope_(m ? m->ctx : nullptr);
     if (!m || S <= 0 || !d_rates || !d_k || !d_state || !d_y) return fail(ESL_ERR_INVALID, "bad argument");
     cudaStream_t s = m->ctx->stream;
     ESL_TRY(grow(m, S));

@@ -34,6 +34,7 @@ extern "C" int esl_solve_many(esl_ctx* const* ctxs, int n_ctx, esl_job* jobs, in
     if (n_jobs == 0) return ESL_OK;
     // symbolic plans once per distinct network, before any thread runs
     {
+        StreamScope stream_scope_(ctxs[0]);
         std::vector<const esl_net*> seen;
         for (int j = 0; j < n_jobs; j++) {
             const esl_net* net = jobs[j].net;

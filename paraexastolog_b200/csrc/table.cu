@@ -157,10 +157,12 @@ __global__ void __launch_bounds__(kMaskWarps * 32) k_flip_masks(DevModel m, uint
 // warps before it, and per group: warp scan of the degrees, edges staged in the warp's
 // shared memory in destination order, coalesced copy out.  No block-wide barrier in the
 // loop.
-template <int MAXN>
+// TOff / TPtr: 32-bit block offsets and column pointers, or 64-bit ones for tables of
+// more than 2^31 - 1 edges (destinations and sources stay 32-bit: n <= 30).
+template <int MAXN, class TOff, class TPtr>
 __global__ void __launch_bounds__(kEmitWarps * 32) k_emit_csc(int n, uint64_t N, const uint32_t* __restrict__ F,
-                                                             const uint32_t* __restrict__ block_offsets,
-                                                             int32_t* __restrict__ indptr, int32_t* __restrict__ rows,
+                                                             const TOff* __restrict__ block_offsets,
+                                                             TPtr* __restrict__ indptr, int32_t* __restrict__ rows,
                                                              int32_t* __restrict__ cols, int64_t nnz) {
     // an edge is staged as (state within the group << 5 | flipped bit)
     __shared__ uint16_t s_stage[kEmitWarps][32 * MAXN];
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(kEmitWarps * 32) k_emit_csc(int n, uint64_t N,
         const uint32_t excl = incl - d;
         const uint32_t gtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
         const uint64_t s = gb + lane;
-        if (s < N) indptr[s] = (int32_t)(out + excl);
+        if (s < N) indptr[s] = (TPtr)(out + excl);
         // destinations ascending: clear bits high -> low, then set bits low -> high
         const uint32_t sv = (uint32_t)s;
         uint32_t down = f[g] & sv, upm = f[g] & ~sv;
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(kEmitWarps * 32) k_emit_csc(int n, uint64_t N,
         out += gtot;
         __syncwarp();
     }
-    if (threadIdx.x == 0 && blk_base < N && blk_base + kTableBlockStates >= N) indptr[N] = (int32_t)nnz;
+    if (threadIdx.x == 0 && blk_base < N && blk_base + kTableBlockStates >= N) indptr[N] = (TPtr)nnz;
 }
 
 // Masks from an arbitrary CSC table whose every edge flips one bit.
@@ -365,19 +367,33 @@ int launch_flip_masks(const DevModel& dm, uint32_t* F, uint32_t* G, uint32_t* bl
     return ESL_OK;
 }
 
-int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
-                    int32_t* cols, int64_t nnz, cudaStream_t s) {
+template <class TOff, class TPtr>
+int launch_emit(int n, const uint32_t* F, const TOff* block_offsets_excl, TPtr* indptr, int32_t* rows, int32_t* cols,
+                int64_t nnz, cudaStream_t s) {
     const uint64_t N = 1ull << n;
     const int64_t blocks = flip_mask_blocks(n);
     ESL_COUNT_LAUNCH();
     if (n <= 16)
-        k_emit_csc<16><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+        k_emit_csc<16, TOff, TPtr><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr,
+                                                                               rows, cols, nnz);
     else if (n <= 24)
-        k_emit_csc<24><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+        k_emit_csc<24, TOff, TPtr><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr,
+                                                                               rows, cols, nnz);
     else
-        k_emit_csc<30><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr, rows, cols, nnz);
+        k_emit_csc<30, TOff, TPtr><<<(unsigned)blocks, kEmitWarps * 32, 0, s>>>(n, N, F, block_offsets_excl, indptr,
+                                                                               rows, cols, nnz);
     ESL_CUDA(cudaGetLastError());
     return ESL_OK;
+}
+
+int launch_emit_csc(int n, const uint32_t* F, const uint32_t* block_offsets_excl, int32_t* indptr, int32_t* rows,
+                    int32_t* cols, int64_t nnz, cudaStream_t s) {
+    return launch_emit<uint32_t, int32_t>(n, F, block_offsets_excl, indptr, rows, cols, nnz, s);
+}
+
+int launch_emit_csc64(int n, const uint32_t* F, const uint64_t* block_offsets_excl, int64_t* indptr, int32_t* rows,
+                      int32_t* cols, int64_t nnz, cudaStream_t s) {
+    return launch_emit<uint64_t, int64_t>(n, F, block_offsets_excl, indptr, rows, cols, nnz, s);
 }
 
 int masks_from_csc(int n, const int32_t* indptr, const int32_t* rows, uint32_t* F, uint32_t* G,
