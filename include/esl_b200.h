@@ -179,6 +179,13 @@ int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* 
  * the batch five times. */
 int esl_net_autotune(esl_ctx* ctx, esl_net* net, int B, const double* d_rates, int R, const double* d_x0,
                      const esl_solve_opts* opts, int* tile_mb, int* two_per_thread, double* ms);
+/* Test hook (no counterpart in the reference): builds the level-sweep plan of `net` afresh,
+ * on the device (host_builder = 0, the builder the solver uses) or with the host reference
+ * builder (1), and writes FNV-1a 64 checksums of its parts to sums[0 .. min(cap, 12)):
+ * rows, desc, in-group and earlier-group predecessor lists (pointers, entries), terminal
+ * predecessor lists (pointers, entries), CTA-local SCC lists (offsets, even counts,
+ * slots) and the group table.  The two builders must agree on all 12. */
+int esl_net_plan_checksums(esl_ctx* ctx, const esl_net* net, int host_builder, uint64_t* sums, int cap);
 /* 1 if the rate set has the zero pattern the net was built for */
 int esl_net_compatible(const esl_net* net, const double* rates, int* compatible);
 

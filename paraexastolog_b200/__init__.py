@@ -103,6 +103,7 @@ def lib():
     L.esl_net_info.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_int)]
     L.esl_net_export.argtypes = [vp, vp, vp, vp, vp, vp]
     L.esl_net_compatible.argtypes = [vp, vp, P(C.c_int)]
+    L.esl_net_plan_checksums.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.esl_net_autotune.argtypes = [vp, vp, C.c_int, vp, C.c_int, vp, P(SolveOpts), P(C.c_int), P(C.c_int),
                                    P(C.c_double)]
     L.esl_solve.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, P(SolveOpts), P(Report)]
@@ -385,6 +386,13 @@ class Net:
         check(lib().esl_net_autotune(self.ctx._h, self._h, r.shape[0], _ptr(r), x.shape[0], _ptr(x), C.byref(o),
                                      C.byref(mb), C.byref(s2), C.byref(ms)))
         return {"tile_mb": mb.value, "two_systems_per_thread": bool(s2.value), "ms": ms.value}
+
+    def plan_checksums(self, host_builder: bool = False) -> np.ndarray:
+        """Checksums of the 12 parts of the level-sweep plan, built afresh on the device
+        or with the host reference builder (test hook)."""
+        out = np.zeros(12, np.uint64)
+        check(lib().esl_net_plan_checksums(self.ctx._h, self._h, int(bool(host_builder)), _ptr(out), 12))
+        return out
 
     def compatible(self, rates: np.ndarray) -> bool:
         rates = np.ascontiguousarray(rates, np.float64)

@@ -696,6 +696,12 @@ int esl_net_export(esl_ctx* ctx, const esl_net* net, int32_t* d_order, int32_t* 
     return ESL_OK;
 }
 
+int esl_net_plan_checksums(esl_ctx* ctx, const esl_net* net, int host_builder, uint64_t* sums, int cap) {
+    StreamScope stream_scope_(ctx);
+    if (!ctx || !net || !sums || cap < 0) return fail(ESL_ERR_INVALID, "bad argument");
+    return plan_checksums_for(ctx, net, host_builder, sums, cap);
+}
+
 int esl_net_compatible(const esl_net* net, const double* rates, int* compatible) {
     if (!net || !rates || !compatible) return fail(ESL_ERR_INVALID, "NULL argument");
     uint32_t up = 0, down = 0;

@@ -310,6 +310,10 @@ int sweep_forward(esl_ctx* ctx, const esl_net* net, int K, int nrhs, const doubl
 int sweep_terminal(esl_ctx* ctx, const esl_net* net, int B, const double* rates, const esl_solve_opts& o, double* Rb,
                    SweepStats& st);
 void free_sweep_workspace(void* w);
+// checksums (FNV-1a 64) of the 12 parts of a freshly built level-sweep plan: rows, desc,
+// ig_ptr, ig_ent, og_ptr, og_ent, tp_ptr, tp_ent, lsc_off, lsc_ne, lsc_slots, group table;
+// host != 0 builds it with the host reference builder instead of the device one
+int plan_checksums_for(esl_ctx* ctx, const esl_net* net, int host, uint64_t* out, int cap);
 // states whose warm start the sweep's grid-wide Krylov groups read (their odd-parity rows)
 int sweep_targets(esl_ctx* ctx, const esl_net* net, std::vector<uint32_t>& states);
 int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, int R, const double* d_x0,

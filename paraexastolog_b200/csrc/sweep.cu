@@ -33,10 +33,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
 #include <nvtx3/nvToolsExt.h>
 
 #include "esl_internal.h"
@@ -1430,14 +1432,10 @@ int build_terminal_plan(const std::vector<int32_t>& order, const std::vector<int
     return ESL_OK;
 }
 
-int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
-    // one builder at a time, so that threads solving the same network share one plan
-    static std::mutex mu;
-    std::lock_guard<std::mutex> lock(mu);
-    if (net->sweep) {
-        out = static_cast<SweepPlan*>(net->sweep);
-        return ESL_OK;
-    }
+// The plan built on the host from copies of the net's arrays: the reference the device
+// builder (build_plan_device) is checked against, bit for bit.
+int build_plan_host(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
+    out = nullptr;
     cudaStream_t s = ctx->stream;
     const auto t_start = std::chrono::steady_clock::now();
     const size_t N = (size_t)net->N;
@@ -1623,6 +1621,429 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     if (debug_on())
         fprintf(stderr, "[esl-sweep] plan: %zu groups, %u slots, %.1f ms on the host\n", P->groups.size(), P->M,
                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    out = P;
+    return ESL_OK;
+}
+
+// ---- the level-sweep plan built on the device --------------------------------------------
+// The same plan as build_plan_host, from the net's device arrays by scans and scatters:
+// transient positions p' = p - TS (the reordering from the first transient SCC), SCCs
+// c' = c - T.  A level group is a run of transient SCCs of one level; a group's slots are
+// its positions, even-parity states first (in position order), then odd.
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+
+// per transient SCC: group-start flag, size; the SCC's first position is marked
+__global__ void k_pl_sccs(int T, int NT, int TS, const int32_t* __restrict__ offsets, const int32_t* __restrict__ levels,
+                          uint32_t* __restrict__ gflag, uint32_t* __restrict__ ssize, uint32_t* __restrict__ pos_head) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= NT) return;
+    const int cc = T + c;
+    gflag[c] = (c == 0 || levels[cc] != levels[cc - 1]) ? 1u : 0u;
+    ssize[c] = (uint32_t)(offsets[cc + 1] - offsets[cc]);
+    pos_head[offsets[cc] - TS] = 1u;
+}
+
+// first SCC of every group (gid_incl: inclusive scan of the group-start flags)
+__global__ void k_pl_gfirst(int NT, const uint32_t* __restrict__ gflag, const uint32_t* __restrict__ gid_incl,
+                            uint32_t* __restrict__ gfirst) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= NT) return;
+    if (gflag[c]) gfirst[gid_incl[c] - 1] = (uint32_t)c;
+    if (c == NT - 1) gfirst[gid_incl[c]] = (uint32_t)NT;
+}
+
+// even-parity flag per transient position (the scan's input has one more, zero, entry)
+__global__ void k_pl_even(uint32_t M, int TS, const int32_t* __restrict__ order, uint32_t* __restrict__ ev) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > M) return;
+    ev[p] = p < M ? ((__popc((uint32_t)order[TS + p]) & 1) == 0 ? 1u : 0u) : 0u;
+}
+
+// Group g (one warp): info[g] = (first position, even rows, odd rows, kind, largest SCC,
+// first SCC, SCCs of >= 2 states, most odd rows of one of them); local groups flag their
+// SCCs of >= 2 states for the CTA-local lists.
+__global__ void k_pl_groups(int T, int TS, const int32_t* __restrict__ offsets, const uint32_t* __restrict__ gid_incl,
+                            int NT, const uint32_t* __restrict__ gfirst, const uint32_t* __restrict__ ssize,
+                            const uint32_t* __restrict__ E, uint32_t* __restrict__ info, uint32_t* __restrict__ qual) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int G = (int)gid_incl[NT - 1];
+    if (warp >= G) return;
+    const uint32_t c0 = gfirst[warp], c1 = gfirst[warp + 1];
+    const uint32_t p0 = (uint32_t)(offsets[T + c0] - TS), p1 = (uint32_t)(offsets[T + c1] - TS);
+    uint32_t mx = 0, n2 = 0, mo = 0;
+    for (uint32_t c = c0 + lane; c < c1; c += 32) {
+        const uint32_t sz = ssize[c];
+        mx = max(mx, sz);
+        if (sz >= 2) {
+            n2++;
+            const uint32_t cs = (uint32_t)(offsets[T + c] - TS), ce = cs + sz;
+            mo = max(mo, sz - (E[ce] - E[cs]));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        mo = max(mo, __shfl_xor_sync(0xFFFFFFFFu, mo, o));
+        n2 += __shfl_xor_sync(0xFFFFFFFFu, n2, o);
+    }
+    const uint32_t kind = mx == 1 ? 0u : (mx <= (uint32_t)kSwLocalMax ? 1u : 2u);
+    for (uint32_t c = c0 + lane; c < c1; c += 32) qual[c] = (kind == 1 && ssize[c] >= 2) ? 1u : 0u;
+    if (lane == 0) {
+        const uint32_t ne = E[p1] - E[p0];
+        uint32_t* o = info + (size_t)warp * 8;
+        o[0] = p0;
+        o[1] = ne;
+        o[2] = (p1 - p0) - ne;
+        o[3] = kind;
+        o[4] = mx;
+        o[5] = c0;
+        o[6] = n2;
+        o[7] = mo;
+    }
+}
+
+// slot of every transient position: rows, slot_of (by state), group of each slot
+__global__ void k_pl_slots(uint32_t M, int TS, const int32_t* __restrict__ order, const uint32_t* __restrict__ F,
+                           const uint32_t* __restrict__ E, const uint32_t* __restrict__ sccpos,
+                           const uint32_t* __restrict__ gid_incl, const uint32_t* __restrict__ info,
+                           uint2* __restrict__ rows, uint32_t* __restrict__ slot_of, uint32_t* __restrict__ slot_grp) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const uint32_t c = sccpos[p] - 1;
+    const uint32_t g = gid_incl[c] - 1;
+    const uint32_t* in = info + (size_t)g * 8;
+    const uint32_t p0 = in[0], ne = in[1];
+    const uint32_t v = (uint32_t)order[TS + p];
+    const bool even = (__popc(v) & 1) == 0;
+    const uint32_t er = E[p] - E[p0];
+    const uint32_t slot = p0 + (even ? er : ne + (p - p0) - er);
+    rows[slot] = make_uint2(v, F[v]);
+    slot_of[v] = slot;
+    slot_grp[slot] = g;
+}
+
+// predecessor entries of a slot: (slot << 6) | rate index, in bit order; COUNT: only
+// count those inside / outside the slot's group
+template <bool COUNT>
+__global__ void k_pl_preds(uint32_t M, const uint2* __restrict__ rows, const uint32_t* __restrict__ G,
+                           const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ slot_grp,
+                           const uint32_t* __restrict__ info, uint32_t* __restrict__ cnt_in, uint32_t* __restrict__ cnt_out,
+                           const uint32_t* __restrict__ ig_ptr, const uint32_t* __restrict__ og_ptr,
+                           uint32_t* __restrict__ ig, uint32_t* __restrict__ og, uint4* __restrict__ desc) {
+    const uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= M) return;
+    const uint2 row = rows[sl];
+    const uint32_t v = row.x;
+    const uint32_t* in = info + (size_t)slot_grp[sl] * 8;
+    const uint32_t gb = in[0], ge = in[0] + in[1] + in[2];
+    uint32_t ci = 0, co = 0;
+    const uint32_t pi0 = COUNT ? 0u : ig_ptr[sl], po0 = COUNT ? 0u : og_ptr[sl];
+    uint32_t g = G[v];
+    while (g) {
+        const int i = __ffs(g) - 1;
+        g &= g - 1;
+        const uint32_t su = slot_of[v ^ (1u << i)];
+        if (su == kNoSlot) continue;  // a terminal state has no edge out of its SCC
+        const bool inside = su >= gb && su < ge;
+        if (!COUNT) {
+            const uint32_t e = (su << kEntShift) | (2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u));
+            if (inside)
+                ig[pi0 + ci] = e;
+            else
+                og[po0 + co] = e;
+        }
+        (inside ? ci : co)++;
+    }
+    if (COUNT) {
+        cnt_in[sl] = ci;
+        cnt_out[sl] = co;
+    } else {
+        desc[sl] = make_uint4(v, row.y, pi0, ci);
+    }
+}
+
+// transient predecessors of the terminal positions
+template <bool COUNT>
+__global__ void k_pl_tpreds(int TS, const int32_t* __restrict__ order, const uint32_t* __restrict__ G,
+                            const uint32_t* __restrict__ slot_of, uint32_t* __restrict__ cnt,
+                            const uint32_t* __restrict__ tp_ptr, uint32_t* __restrict__ tp) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= TS) return;
+    const uint32_t v = (uint32_t)order[p];
+    uint32_t g = G[v], c = 0;
+    const uint32_t b = COUNT ? 0u : tp_ptr[p];
+    while (g) {
+        const int i = __ffs(g) - 1;
+        g &= g - 1;
+        const uint32_t su = slot_of[v ^ (1u << i)];
+        if (su == kNoSlot) continue;
+        if (!COUNT) tp[b + c] = (su << kEntShift) | (2u * (uint32_t)i + (((v >> i) & 1u) ^ 1u));
+        c++;
+    }
+    if (COUNT) cnt[p] = c;
+}
+
+// per group: first local-SCC list entry and in-group predecessor entries
+__global__ void k_pl_gtail(int G, const uint32_t* __restrict__ info, const uint32_t* __restrict__ qidx,
+                           const uint32_t* __restrict__ ig_ptr, uint32_t* __restrict__ gtail) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const uint32_t* in = info + (size_t)g * 8;
+    const uint32_t b = in[0], e = in[0] + in[1] + in[2];
+    gtail[2 * g] = qidx[in[5]];
+    gtail[2 * g + 1] = ig_ptr[e] - ig_ptr[b];
+}
+
+// CTA-local SCC lists: slots of each flagged SCC, even-parity ones first
+__global__ void k_pl_lsc(uint32_t M, int T, int TS, const int32_t* __restrict__ offsets, const int32_t* __restrict__ order,
+                         const uint32_t* __restrict__ E, const uint32_t* __restrict__ sccpos,
+                         const uint32_t* __restrict__ qual, const uint32_t* __restrict__ qidx,
+                         const uint32_t* __restrict__ qoff, const uint32_t* __restrict__ ssize,
+                         const uint32_t* __restrict__ slot_of, uint32_t* __restrict__ lsc_off,
+                         uint32_t* __restrict__ lsc_ne, uint32_t* __restrict__ lsc_slots, uint32_t Q) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const uint32_t c = sccpos[p] - 1;
+    if (!qual[c]) return;
+    const uint32_t cs = (uint32_t)(offsets[T + c] - TS), sz = ssize[c];
+    const uint32_t ne = E[cs + sz] - E[cs];
+    const uint32_t v = (uint32_t)order[TS + p];
+    const bool even = (__popc(v) & 1) == 0;
+    const uint32_t er = E[p] - E[cs];
+    const uint32_t local = even ? er : ne + (p - cs) - er;
+    lsc_slots[qoff[c] + local] = slot_of[v];
+    if (p == cs) {
+        const uint32_t j = qidx[c];
+        lsc_off[j] = qoff[c];
+        lsc_ne[j] = ne;
+        if (j + 1 == Q) lsc_off[Q] = qoff[c] + sz;
+    }
+}
+
+// qsize = size of a flagged SCC, else 0 (one more, zero, entry for the scan)
+__global__ void k_pl_qsize(int NT, const uint32_t* __restrict__ qual, const uint32_t* __restrict__ ssize,
+                           uint32_t* __restrict__ qsize) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > NT) return;
+    qsize[c] = (c < NT && qual[c]) ? ssize[c] : 0u;
+}
+
+// exclusive scan of n + 1 counts (the last one 0) into out[0 .. n], on the stream
+int scan_excl(DevBuf<uint8_t>& tmp, const uint32_t* in, uint32_t* out, uint32_t n1, cudaStream_t s) {
+    size_t bytes = 0;
+    ESL_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int64_t)n1, s));
+    if (tmp.n < bytes) ESL_TRY(tmp.alloc(bytes));
+    ESL_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, (int64_t)n1, s));
+    return ESL_OK;
+}
+int scan_incl(DevBuf<uint8_t>& tmp, const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t s) {
+    size_t bytes = 0;
+    ESL_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, (int64_t)n, s));
+    if (tmp.n < bytes) ESL_TRY(tmp.alloc(bytes));
+    ESL_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, in, out, (int64_t)n, s));
+    return ESL_OK;
+}
+
+inline unsigned nblk(uint64_t n) { return (unsigned)std::max<uint64_t>(1, (n + 255) / 256); }
+
+int build_plan_device(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
+    out = nullptr;
+    cudaStream_t s = ctx->stream;
+    const auto t_start = std::chrono::steady_clock::now();
+    const size_t N = (size_t)net->N;
+    const int n_sccs = net->n_sccs, T = net->T, TS = net->term_states;
+    const int NT = n_sccs - T;
+    const uint32_t M = (uint32_t)(N - (size_t)TS);
+    std::unique_ptr<SweepPlan> P(new SweepPlan());
+    P->TS = TS;
+    P->M = M;
+    DevBuf<uint8_t> tmp;
+    DevBuf<uint32_t> slot_of;
+    ESL_TRY(slot_of.alloc(N));
+    ESL_CUDA(cudaMemsetAsync(slot_of.get(), 0xFF, N * 4, s));
+    const int32_t* order = net->order.get();
+    const int32_t* offsets = net->offsets.get();
+    std::vector<uint32_t> h_info, h_tail;
+    uint32_t G = 0, tot[5] = {0, 0, 0, 0, 0};
+    if (M > 0) {
+        DevBuf<uint32_t> gflag, gid, ssize, gfirst, info, qual, qidx, qsize, qoff, pos_head, sccpos, ev, E, slot_grp,
+            cnt_in, cnt_out, gtail;
+        ESL_TRY(gflag.alloc(NT));
+        ESL_TRY(gid.alloc(NT));
+        ESL_TRY(ssize.alloc(NT));
+        ESL_TRY(gfirst.alloc(NT + 1));
+        ESL_TRY(info.alloc((size_t)NT * 8));
+        ESL_TRY(qual.alloc(NT + 1));
+        ESL_TRY(qidx.alloc(NT + 1));
+        ESL_TRY(qsize.alloc(NT + 1));
+        ESL_TRY(qoff.alloc(NT + 1));
+        ESL_TRY(pos_head.alloc(M));
+        ESL_TRY(sccpos.alloc(M));
+        ESL_TRY(ev.alloc((size_t)M + 1));
+        ESL_TRY(E.alloc((size_t)M + 1));
+        ESL_TRY(slot_grp.alloc(M));
+        ESL_TRY(cnt_in.alloc((size_t)M + 1));
+        ESL_TRY(cnt_out.alloc((size_t)M + 1));
+        ESL_CUDA(cudaMemsetAsync(pos_head.get(), 0, (size_t)M * 4, s));
+        ESL_CUDA(cudaMemsetAsync(qual.get(), 0, (size_t)(NT + 1) * 4, s));
+        ESL_COUNT_LAUNCH();
+        k_pl_sccs<<<nblk(NT), 256, 0, s>>>(T, NT, TS, offsets, net->levels.get(), gflag.get(), ssize.get(),
+                                           pos_head.get());
+        ESL_TRY(scan_incl(tmp, gflag.get(), gid.get(), (uint32_t)NT, s));
+        ESL_COUNT_LAUNCH();
+        k_pl_gfirst<<<nblk(NT), 256, 0, s>>>(NT, gflag.get(), gid.get(), gfirst.get());
+        ESL_COUNT_LAUNCH();
+        k_pl_even<<<nblk((uint64_t)M + 1), 256, 0, s>>>(M, TS, order, ev.get());
+        ESL_TRY(scan_excl(tmp, ev.get(), E.get(), M + 1, s));
+        ESL_TRY(scan_incl(tmp, pos_head.get(), sccpos.get(), M, s));
+        ESL_COUNT_LAUNCH();
+        k_pl_groups<<<nblk((uint64_t)NT * 32), 256, 0, s>>>(T, TS, offsets, gid.get(), NT, gfirst.get(), ssize.get(),
+                                                            E.get(), info.get(), qual.get());
+        ESL_CUDA(cudaGetLastError());
+        // CTA-local lists: index and slot offset of every flagged SCC
+        ESL_TRY(scan_excl(tmp, qual.get(), qidx.get(), (uint32_t)NT + 1, s));
+        ESL_COUNT_LAUNCH();
+        k_pl_qsize<<<nblk((uint64_t)NT + 1), 256, 0, s>>>(NT, qual.get(), ssize.get(), qsize.get());
+        ESL_TRY(scan_excl(tmp, qsize.get(), qoff.get(), (uint32_t)NT + 1, s));
+        ESL_TRY(P->rows.alloc(M));
+        ESL_COUNT_LAUNCH();
+        k_pl_slots<<<nblk(M), 256, 0, s>>>(M, TS, order, net->F.get(), E.get(), sccpos.get(), gid.get(), info.get(),
+                                           P->rows.get(), slot_of.get(), slot_grp.get());
+        ESL_COUNT_LAUNCH();
+        k_pl_preds<true><<<nblk(M), 256, 0, s>>>(M, P->rows.get(), net->G.get(), slot_of.get(), slot_grp.get(),
+                                                 info.get(), cnt_in.get(), cnt_out.get(), nullptr, nullptr, nullptr,
+                                                 nullptr, nullptr);
+        ESL_CUDA(cudaMemsetAsync(cnt_in.get() + M, 0, 4, s));
+        ESL_CUDA(cudaMemsetAsync(cnt_out.get() + M, 0, 4, s));
+        ESL_TRY(P->ig_ptr.alloc((size_t)M + 1));
+        ESL_TRY(P->og_ptr.alloc((size_t)M + 1));
+        ESL_TRY(scan_excl(tmp, cnt_in.get(), P->ig_ptr.get(), M + 1, s));
+        ESL_TRY(scan_excl(tmp, cnt_out.get(), P->og_ptr.get(), M + 1, s));
+        ESL_CUDA(cudaGetLastError());
+        // the group count and the group table
+        ESL_CUDA(cudaMemcpyAsync(&G, gid.get() + NT - 1, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        ESL_TRY(gtail.alloc((size_t)G * 2));
+        ESL_COUNT_LAUNCH();
+        k_pl_gtail<<<nblk(G), 256, 0, s>>>((int)G, info.get(), qidx.get(), P->ig_ptr.get(), gtail.get());
+        ESL_CUDA(cudaGetLastError());
+        h_info.resize((size_t)G * 8);
+        h_tail.resize((size_t)G * 2);
+        ESL_CUDA(cudaMemcpyAsync(h_info.data(), info.get(), (size_t)G * 32, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(h_tail.data(), gtail.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(&tot[0], P->ig_ptr.get() + M, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(&tot[1], P->og_ptr.get() + M, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(&tot[2], qidx.get() + NT, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(&tot[3], qoff.get() + NT, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        ESL_TRY(P->ig_ent.alloc(std::max<uint32_t>(tot[0], 1)));
+        ESL_TRY(P->og_ent.alloc(std::max<uint32_t>(tot[1], 1)));
+        ESL_TRY(P->desc.alloc(M));
+        ESL_COUNT_LAUNCH();
+        k_pl_preds<false><<<nblk(M), 256, 0, s>>>(M, P->rows.get(), net->G.get(), slot_of.get(), slot_grp.get(),
+                                                  info.get(), nullptr, nullptr, P->ig_ptr.get(), P->og_ptr.get(),
+                                                  P->ig_ent.get(), P->og_ent.get(), P->desc.get());
+        ESL_TRY(P->lsc_off.alloc((size_t)tot[2] + 1));
+        ESL_TRY(P->lsc_ne.alloc(std::max<uint32_t>(tot[2], 1)));
+        ESL_TRY(P->lsc_slots.alloc(std::max<uint32_t>(tot[3], 1)));
+        ESL_CUDA(cudaMemsetAsync(P->lsc_off.get(), 0, 4, s));
+        if (tot[2] > 0) {
+            ESL_COUNT_LAUNCH();
+            k_pl_lsc<<<nblk(M), 256, 0, s>>>(M, T, TS, offsets, order, E.get(), sccpos.get(), qual.get(), qidx.get(),
+                                             qoff.get(), ssize.get(), slot_of.get(), P->lsc_off.get(), P->lsc_ne.get(),
+                                             P->lsc_slots.get(), tot[2]);
+        }
+        ESL_CUDA(cudaGetLastError());
+    } else {
+        ESL_TRY(P->rows.alloc(1));
+        ESL_TRY(P->desc.alloc(1));
+        ESL_TRY(P->ig_ptr.alloc(1));
+        ESL_TRY(P->og_ptr.alloc(1));
+        ESL_TRY(P->ig_ent.alloc(1));
+        ESL_TRY(P->og_ent.alloc(1));
+        ESL_TRY(P->lsc_off.alloc(1));
+        ESL_TRY(P->lsc_ne.alloc(1));
+        ESL_TRY(P->lsc_slots.alloc(1));
+        ESL_CUDA(cudaMemsetAsync(P->ig_ptr.get(), 0, 4, s));
+        ESL_CUDA(cudaMemsetAsync(P->og_ptr.get(), 0, 4, s));
+        ESL_CUDA(cudaMemsetAsync(P->lsc_off.get(), 0, 4, s));
+    }
+    // transient predecessors of the terminal positions
+    {
+        DevBuf<uint32_t> cnt;
+        ESL_TRY(cnt.alloc((size_t)TS + 1));
+        ESL_TRY(P->tp_ptr.alloc((size_t)TS + 1));
+        ESL_CUDA(cudaMemsetAsync(cnt.get(), 0, ((size_t)TS + 1) * 4, s));
+        if (TS > 0) {
+            ESL_COUNT_LAUNCH();
+            k_pl_tpreds<true><<<nblk(TS), 256, 0, s>>>(TS, order, net->G.get(), slot_of.get(), cnt.get(), nullptr,
+                                                       nullptr);
+        }
+        ESL_TRY(scan_excl(tmp, cnt.get(), P->tp_ptr.get(), (uint32_t)TS + 1, s));
+        ESL_CUDA(cudaMemcpyAsync(&tot[4], P->tp_ptr.get() + TS, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        ESL_TRY(P->tp_ent.alloc(std::max<uint32_t>(tot[4], 1)));
+        if (TS > 0) {
+            ESL_COUNT_LAUNCH();
+            k_pl_tpreds<false><<<nblk(TS), 256, 0, s>>>(TS, order, net->G.get(), slot_of.get(), nullptr,
+                                                        P->tp_ptr.get(), P->tp_ent.get());
+        }
+        ESL_CUDA(cudaGetLastError());
+    }
+    // the group table on the host
+    for (uint32_t g = 0; g < G; g++) {
+        const uint32_t* in = &h_info[(size_t)g * 8];
+        SwGroup gr{};
+        gr.beg = in[0];
+        gr.ne = in[1];
+        gr.no = in[2];
+        gr.kind = (int)in[3];
+        gr.max_scc = (int)in[4];
+        gr.term = -1;
+        if (gr.kind == 1) {
+            gr.scc0 = h_tail[2 * g];
+            gr.nscc = in[6];
+            gr.max_odd = (int)in[7];
+        }
+        gr.nin = h_tail[2 * g + 1];
+        P->max_rows = std::max(P->max_rows, gr.ne + gr.no);
+        P->max_even = std::max(P->max_even, gr.ne);
+        P->max_odd = std::max(P->max_odd, gr.no);
+        if (gr.kind == 1) {
+            P->max_even_local = std::max(P->max_even_local, gr.ne);
+            P->max_odd_local = std::max(P->max_odd_local, gr.no);
+        }
+        P->groups.push_back(gr);
+    }
+    ESL_CUDA(cudaStreamSynchronize(s));
+    // the terminal plan, for networks with terminal SCCs above kDenseTerminalMax states
+    if (net->max_terminal > kDenseTerminalMax) {
+        std::vector<int32_t> h_order(TS), h_off(T + 1);
+        std::vector<uint32_t> hF(N), hG(N);
+        ESL_CUDA(cudaMemcpyAsync(h_order.data(), order, (size_t)TS * 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(h_off.data(), offsets, (size_t)(T + 1) * 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(hF.data(), net->F.get(), N * 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(hG.data(), net->G.get(), N * 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        ESL_TRY(build_terminal_plan(h_order, h_off, T, hF, hG, s, P->term));
+    }
+    if (debug_on())
+        fprintf(stderr, "[esl-sweep] plan: %zu groups, %u slots, %.1f ms on the device\n", P->groups.size(), P->M,
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    out = P.release();
+    return ESL_OK;
+}
+
+int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
+    // one builder at a time, so that threads solving the same network share one plan
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (net->sweep) {
+        out = static_cast<SweepPlan*>(net->sweep);
+        return ESL_OK;
+    }
+    SweepPlan* P = nullptr;
+    ESL_TRY(build_plan_device(ctx, net, P));
     esl_net* mnet = const_cast<esl_net*>(net);
     mnet->sweep = P;
     mnet->sweep_free = free_plan_sweep;
@@ -1712,7 +2133,81 @@ bool compact_on() {
     return on;
 }
 
+// FNV-1a 64 over n 32-bit words of a device array
+int dev_checksum(const void* d, size_t words, cudaStream_t s, uint64_t& h) {
+    std::vector<uint32_t> v(words);
+    if (words) {
+        ESL_CUDA(cudaMemcpyAsync(v.data(), d, words * 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+    }
+    h = 1469598103934665603ull;
+    for (uint32_t w : v) {
+        h ^= w;
+        h *= 1099511628211ull;
+    }
+    return ESL_OK;
+}
+
+int plan_checksums(esl_ctx* ctx, const SweepPlan& P, uint64_t (&h)[12]) {
+    cudaStream_t s = ctx->stream;
+    uint32_t ig = 0, og = 0, tp = 0, Q = 0, L = 0;
+    for (const SwGroup& g : P.groups)
+        if (g.kind == 1) Q += g.nscc;
+    if (P.M) {
+        ESL_CUDA(cudaMemcpyAsync(&ig, P.ig_ptr.get() + P.M, 4, cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaMemcpyAsync(&og, P.og_ptr.get() + P.M, 4, cudaMemcpyDeviceToHost, s));
+    }
+    ESL_CUDA(cudaMemcpyAsync(&tp, P.tp_ptr.get() + P.TS, 4, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaMemcpyAsync(&L, P.lsc_off.get() + Q, 4, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    ESL_TRY(dev_checksum(P.rows.get(), (size_t)P.M * 2, s, h[0]));
+    ESL_TRY(dev_checksum(P.desc.get(), (size_t)P.M * 4, s, h[1]));
+    ESL_TRY(dev_checksum(P.ig_ptr.get(), P.M ? (size_t)P.M + 1 : 0, s, h[2]));
+    ESL_TRY(dev_checksum(P.ig_ent.get(), ig, s, h[3]));
+    ESL_TRY(dev_checksum(P.og_ptr.get(), P.M ? (size_t)P.M + 1 : 0, s, h[4]));
+    ESL_TRY(dev_checksum(P.og_ent.get(), og, s, h[5]));
+    ESL_TRY(dev_checksum(P.tp_ptr.get(), (size_t)P.TS + 1, s, h[6]));
+    ESL_TRY(dev_checksum(P.tp_ent.get(), tp, s, h[7]));
+    ESL_TRY(dev_checksum(P.lsc_off.get(), (size_t)Q + 1, s, h[8]));
+    ESL_TRY(dev_checksum(P.lsc_ne.get(), Q, s, h[9]));
+    ESL_TRY(dev_checksum(P.lsc_slots.get(), L, s, h[10]));
+    uint64_t g = 1469598103934665603ull;
+    auto mix = [&](uint64_t x) {
+        g ^= x;
+        g *= 1099511628211ull;
+    };
+    for (const SwGroup& gr : P.groups) {
+        mix(gr.beg);
+        mix(gr.ne);
+        mix(gr.no);
+        mix((uint64_t)gr.kind);
+        mix((uint64_t)gr.max_scc);
+        mix(gr.kind == 1 ? gr.scc0 : 0);
+        mix(gr.kind == 1 ? gr.nscc : 0);
+        mix(gr.kind == 1 ? (uint64_t)gr.max_odd : 0);
+        mix(gr.nin);
+    }
+    mix(P.max_rows);
+    mix(P.max_even);
+    mix(P.max_odd);
+    mix(P.max_even_local);
+    mix(P.max_odd_local);
+    h[11] = g;
+    return ESL_OK;
+}
+
 }  // namespace
+
+int plan_checksums_for(esl_ctx* ctx, const esl_net* net, int host, uint64_t* out, int cap) {
+    if (!sweep_supported(net)) return fail(ESL_ERR_TOO_LARGE, "level sweep supports at most 26 nodes");
+    SweepPlan* P = nullptr;
+    ESL_TRY(host ? build_plan_host(ctx, net, P) : build_plan_device(ctx, net, P));
+    std::unique_ptr<SweepPlan> keep(P);
+    uint64_t h[12];
+    ESL_TRY(plan_checksums(ctx, *P, h));
+    for (int i = 0; i < cap && i < 12; i++) out[i] = h[i];
+    return ESL_OK;
+}
 
 void free_sweep_workspace(void* w) { delete static_cast<Workspace*>(w); }
 

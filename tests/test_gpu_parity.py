@@ -329,3 +329,19 @@ def test_autotune_keeps_results(esl, ctx):
     assert pick["tile_mb"] in (16, 48, 128) and pick["ms"] > 0
     after = esl.solve_batch(ctx, net, rates, x0, method=esl.METHOD_DIRECT, tol=1e-12).x_inf.cpu().numpy()
     assert np.abs(after - before).sum(-1).max() <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["rand0", "canal12", "prec12", "tiny3", "bench20"])
+def test_device_plan_equals_host_plan(esl, ctx, name):
+    """The level-sweep plan the solver builds on the device equals, part for part, the
+    one the host reference builder makes from copies of the net's arrays."""
+    if name == "bench20":
+        text = synth.config_learned(n_rate_sets=1).networks[0].bnet
+    else:
+        text = dict(_nets())[name]
+    m = esl.Model.parse(text)
+    r = _rates(m.n, 9)
+    net = esl.Net.build(ctx, m, r)
+    dev = net.plan_checksums(host_builder=False)
+    host = net.plan_checksums(host_builder=True)
+    assert np.array_equal(dev, host), (dev, host)
