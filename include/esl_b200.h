@@ -67,6 +67,8 @@ typedef struct esl_report {
     int converged;         /* 1 if every system met tol */
     int fallback_systems;  /* systems the level sweep handed to the block forward solve */
     int dense_lu_systems;  /* (system, level group) pairs solved by the dense LU of their SCC blocks */
+    int absorption_by_sweep; /* 1 if L (d_L) missed its tolerance in the backward solve and was
+                                computed by forward level sweeps instead */
 } esl_report;
 
 const char* esl_last_error(void);

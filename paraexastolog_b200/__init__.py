@@ -47,7 +47,8 @@ class SolveOpts(C.Structure):
 
 class Report(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("relres", C.c_double), ("converged", C.c_int),
-                ("fallback_systems", C.c_int), ("dense_lu_systems", C.c_int)]
+                ("fallback_systems", C.c_int), ("dense_lu_systems", C.c_int),
+                ("absorption_by_sweep", C.c_int)]
 
 
 class Job(C.Structure):

@@ -57,6 +57,14 @@ struct KState {
     double r0v, ts, tt, r0r, rr;
     double rnorm2_true, bnorm2, target2, prev_r2, rnorm2_trial;
     int done, iters, breakdown, pad, noimp, total_iters;
+    // the last inner solve's exit, kept for the debug report: breakdown code, its
+    // iterations, and r0.v / r.r when it stopped
+    int last_breakdown, last_iters;
+    double last_r0v, last_rr;
+    // inner solves restarted after a breakdown or a correction that did not lower the
+    // true residual; from the first, the shadow residual r0 is no longer r itself but r
+    // plus a dense positive vector (k_inner_start)
+    int shadow;
 };
 
 // A system whose true FP64 residual stops improving (a refinement step no longer
@@ -301,21 +309,48 @@ __global__ void __launch_bounds__(kT) k_schur_diag(Layout L, const double* __res
 }
 
 // ---- BiCGStab vector updates ------------------------------------------------------
-// start of an inner solve: r = r0 = (T) r64, d = 0, p = v = 0, scalars reset
+// start of an inner solve: r = (T) r64, d = 0, p = v = 0, scalars reset.  The shadow
+// residual is r0 = r, except in a system restarted after a breakdown or a useless
+// correction (st.shadow > 0): there domain row h gets r0_h = r_h + c_h |r| / sqrt(rows),
+// c_h in [0.5, 1.5) from a hash of (h, system, restart), and rho = r0.r is summed here
+// (k_outer_check left it at 0).  Why: when the transient part is acyclic, the Jacobi-
+// scaled Schur complement is I - N with N nilpotent, and a shadow residual with the
+// support of r can be orthogonal to the whole Krylov space: in one backward system of
+// the 15-node kras network with uniform rates (32,768 singleton SCCs), r0.v fell to
+// 1e-16 |r0||v| at the second iteration of every refinement round, with r0 = r and with
+// r0 = r scaled row by row alike; the dense shadow converges in 8 iterations.  Any r0
+// with r0.r != 0 is a valid BiCGStab shadow residual.
 template <class T>
-__global__ void k_inner_start(Layout L, const double* __restrict__ r64, T* __restrict__ r, T* __restrict__ r0,
-                              T* __restrict__ d, T* __restrict__ ph, T* __restrict__ v, const KState* __restrict__ st) {
+__global__ void __launch_bounds__(kT) k_inner_start(Layout L, const double* __restrict__ r64, T* __restrict__ r,
+                                                    T* __restrict__ r0, T* __restrict__ d, T* __restrict__ ph,
+                                                    T* __restrict__ v, KState* __restrict__ st) {
     const int k = sys_index(L);
     if (st[k].done) return;
-    uint32_t h;
-    if (!row_h(L, 1, h)) return;
-    size_t i = (size_t)k * L.ld + h;
-    T val = (T)r64[i];
-    r[i] = val;
-    r0[i] = val;
-    d[i] = 0;
-    ph[i] = 0;
-    v[i] = 0;
+    const int shadow = st[k].shadow;
+    uint32_t h = 0;
+    const bool valid = row_h(L, 1, h);
+    double a = 0.0;
+    if (valid) {
+        size_t i = (size_t)k * L.ld + h;
+        T val = (T)r64[i];
+        r[i] = val;
+        T sv = val;
+        if (shadow && (L.M1[h] & kDomainBit)) {
+            uint32_t x = h * 0x9E3779B1u ^ (uint32_t)k * 0x85EBCA77u ^ (uint32_t)shadow * 0xC2B2AE3Du;
+            x ^= x >> 15;
+            x *= 0x2C1B3C6Du;
+            x ^= x >> 12;
+            const double rows = (double)(L.list1 ? L.n1 : L.H);
+            const double c = 0.5 + (double)(x >> 8) * (1.0 / 16777216.0);
+            sv = (T)((double)val + c * sqrt(st[k].rnorm2_true / rows));
+            a = (double)sv * (double)val;
+        }
+        r0[i] = sv;
+        d[i] = 0;
+        ph[i] = 0;
+        v[i] = 0;
+    }
+    if (shadow) block_sum2(a, 0.0, &st[k].rho, nullptr);
 }
 
 template <class T>
@@ -424,10 +459,15 @@ __global__ void k_outer_check(int K, KState* st, double tol2, double inner_rel2,
     bool stalled = outer > 0 && (s.noimp || s.rnorm2_true > 0.25 * s.prev_r2) &&
                    s.rnorm2_true <= kAcceptRel * kAcceptRel * s.bnorm2;
     s.prev_r2 = s.rnorm2_true;
+    s.last_breakdown = s.breakdown;
+    s.last_iters = s.iters;
+    s.last_r0v = s.r0v;
+    s.last_rr = s.rr;
     s.done = (conv || stalled || s.total_iters >= budget) ? 1 : 0;
     if (!s.done) {
         atomicAdd(n_active, 1);
-        s.rho = s.rnorm2_true;  // r0 = r at the start: rho = r0.r
+        if (s.breakdown || s.noimp) s.shadow++;
+        s.rho = s.shadow ? 0.0 : s.rnorm2_true;  // r0 = r: rho = r0.r; else k_inner_start sums it
         s.alpha = s.omega = 1.0;
         s.beta = 0.0;
         s.r0v = 0.0;
@@ -973,6 +1013,7 @@ struct SolveOut {
     std::vector<double> sys_relres;  // per system, from the last Krylov solve
     int fallback_systems = 0;        // systems the level sweep handed to the block forward solve
     int dense_systems = 0;           // (system, level group) pairs solved by the dense LU fallback
+    bool absorption_by_sweep = false;  // L came from forward sweeps after the backward solve missed
 };
 
 void fill_report(esl_report* rep, const SolveOut& agg, bool converged) {
@@ -983,6 +1024,7 @@ void fill_report(esl_report* rep, const SolveOut& agg, bool converged) {
     rep->converged = converged ? 1 : 0;
     rep->fallback_systems = agg.fallback_systems;
     rep->dense_lu_systems = agg.dense_systems;
+    rep->absorption_by_sweep = agg.absorption_by_sweep ? 1 : 0;
 }
 
 // Solves the K systems whose rhs halves are in (bE, bO); solution in x64 (odd) and zE (even).
@@ -1064,8 +1106,11 @@ int krylov_solve(esl_ctx* ctx, Workspace& ws, const Layout& L, const double* rat
                 double rel = h_st[k].bnorm2 > 0 ? std::sqrt(h_st[k].rnorm2_true / h_st[k].bnorm2) : 0.0;
                 if (k >= 2 && rel <= tol) continue;
                 shown++;
-                fprintf(stderr, "[esl] outer %d sys %d/%d relres %.3e b2 %.3e inner64 %d breakdown %d iters %d\n", outer,
-                        k, K, rel, h_st[k].bnorm2, (int)inner64, h_st[k].breakdown, h_st[k].iters);
+                fprintf(stderr,
+                        "[esl] outer %d sys %d/%d relres %.3e b2 %.3e inner64 %d last inner: breakdown %d iters %d "
+                        "r0v %.3e rr %.3e\n",
+                        outer, k, K, rel, h_st[k].bnorm2, (int)inner64, h_st[k].last_breakdown, h_st[k].last_iters,
+                        h_st[k].last_r0v, h_st[k].last_rr);
             }
         }
         if (active == 0 || outer >= o.max_refine) break;
@@ -1980,6 +2025,7 @@ int solve_batch(esl_ctx* ctx, const esl_net* net, int B, const double* d_rates, 
             } else if (rc == ESL_ERR_NOT_CONVERGED && sweep_supported(net)) {
                 if (debug_enabled()) fprintf(stderr, "[esl] L: backward solve missed its tolerance, forward sweep\n");
                 ESL_TRY(absorption_by_sweep(ctx, ws, net, d_rates, o, d_L));
+                agg.absorption_by_sweep = true;
             } else {
                 return rc;
             }
