@@ -218,12 +218,14 @@ __device__ __forceinline__ bool sw_skip(const SwArgs& a, int k) {
 }
 
 // acc[j] += sum over the predecessor entries ent[p0 .. p0 + cnt) of a row of
-// rate(entry) * X[ent_slot(entry) - base][system j], in entry order.  All 32 lanes of a
+// rate(entry) * X[ent_slot(entry) - base][system j], in entry order.  With MASK false,
+// systems with act[j] == false accumulate whatever their rows hold (their acc must then
+// be left unused by the caller); with MASK true they add zero.  All 32 lanes of a
 // warp handle the same row, so the row's entries (at most n <= 26) arrive in one
 // coalesced load and are broadcast by shuffles, and the gathers are issued four entries
 // at a time.  Every lane of the warp must call it; systems with act[j] == false load
 // nothing.
-template <int S, class TC, class TX>
+template <int S, class TC, class TX, bool MASK = true>
 __device__ __forceinline__ void sw_gathers_m(const TC* s, const Tile& t, int Kp, uint32_t mine, int cnt,
                                              const TX* __restrict__ X, uint32_t base, const bool (&act)[S],
                                              TC (&acc)[S]) {
@@ -255,7 +257,7 @@ __device__ __forceinline__ void sw_gathers_m(const TC* s, const Tile& t, int Kp,
             TC r[S];
             load_s<S, TC>(sk + ent_rate(e[u]) * t.KT, r);
 #pragma unroll
-            for (int q = 0; q < S; q++) acc[q] += r[q] * (act[q] ? (TC)x[u][q] : (TC)0);
+            for (int q = 0; q < S; q++) acc[q] += r[q] * ((!MASK || act[q]) ? (TC)x[u][q] : (TC)0);
         }
     }
     for (; j < cnt; j++) {
@@ -271,17 +273,17 @@ __device__ __forceinline__ void sw_gathers_m(const TC* s, const Tile& t, int Kp,
         TC r[S];
         load_s<S, TC>(sk + ent_rate(e) * t.KT, r);
 #pragma unroll
-        for (int q = 0; q < S; q++) acc[q] += r[q] * (act[q] ? (TC)x[q] : (TC)0);
+        for (int q = 0; q < S; q++) acc[q] += r[q] * ((!MASK || act[q]) ? (TC)x[q] : (TC)0);
     }
 }
 
-template <int S, class TC, class TX>
+template <int S, class TC, class TX, bool MASK = true>
 __device__ __forceinline__ void sw_gathers(const TC* s, const Tile& t, int Kp, const uint32_t* __restrict__ ent,
                                            uint32_t p0, int cnt, const TX* __restrict__ X, uint32_t base,
                                            const bool (&act)[S], TC (&acc)[S]) {
     const int lane = threadIdx.x & 31;
     const uint32_t mine = lane < cnt ? __ldg(ent + p0 + lane) : 0u;
-    sw_gathers_m<S, TC, TX>(s, t, Kp, mine, cnt, X, base, act, acc);
+    sw_gathers_m<S, TC, TX, MASK>(s, t, Kp, mine, cnt, X, base, act, acc);
 }
 
 template <class TC, class TX>
@@ -421,7 +423,8 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim(SwArgs a, const double* __rest
         TC acc[S];
 #pragma unroll
         for (int q = 0; q < S; q++) acc[q] = (C && act[q]) ? (TC)C[idx + q] : (TC)0;
-        if (X) sw_gathers<S, TC, TX>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, X, obase, act, acc);
+        // acc of an inactive system is never stored: no masking in the gathers
+        if (X) sw_gathers<S, TC, TX, false>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, X, obase, act, acc);
         if (sizeof(TC) == 8 && a.IQe) {
 #pragma unroll
             for (int q = 0; q < S; q++)
@@ -489,7 +492,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
             T flow[S];
 #pragma unroll
             for (int q = 0; q < S; q++) flow[q] = 0;
-            sw_gathers<S, T, T>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, W, a.beg, act, flow);
+            sw_gathers<S, T, T, false>(s_rate, t, a.Kp, a.ig_ent, d.z, (int)d.w, W, a.beg, act, flow);
             T qv[S];
             if (MODE != 0) {
                 if (sizeof(T) == 8 && a.Qo) {
@@ -576,6 +579,172 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
         for (int q = 0; q < S; q++) v[0][q] = d0[q];
         double* const dst[1] = {acc0};
         sw_reduce<1, S>(v, dst, t, a.K);
+    }
+}
+
+// ---- paired-row Schur operator for 32-system tiles ---------------------------------------
+// The largest level groups run 32-system tiles (their gathered slice must stay in L2), and
+// with one system per lane a warp spends ~13 instructions per system and predecessor entry
+// on the entry shuffle, the address, the load, the rate look-up and the select.  Here a
+// half warp serves one row and each lane two adjacent systems, so a warp runs two rows at
+// once and every instruction of the gather loop serves four (row, system) pairs: the
+// row value and the rate are 16-byte loads.  The two rows' entry counts differ; the loop
+// runs to the larger count and the other half's gathers are predicated off.  FP64, no
+// deflation, out-rate sums from SwArgs::Qo / IQe.  Tile layout: KT = 32, S = 2, TR = 16
+// (tile_of<2>(32): rsub = threadIdx.x / 16, lane = threadIdx.x % 16).
+
+// entry j (< 32) of this half warp's row, from the row's first 16 entries (m0, lane l16
+// holds entry l16) or the next 16 (m1); j is warp-uniform
+__device__ __forceinline__ uint32_t pr_entry(uint32_t m0, uint32_t m1, int j) {
+    return j < 16 ? __shfl_sync(0xffffffffu, m0, j, 16) : __shfl_sync(0xffffffffu, m1, j - 16, 16);
+}
+
+// acc[q] += sum over this half warp's row's cnt entries of rate(entry) * X[entry row]
+// for this lane's two systems; cmax = the larger count of the warp's two rows.  The sums
+// of inactive systems take whatever their rows hold and are never stored.
+__device__ __forceinline__ void pr_gathers(const double* s_rate, const Tile& t, int Kp, uint32_t m0, uint32_t m1,
+                                           int cnt, int cmax, const double* __restrict__ X, uint32_t base,
+                                           bool any, double (&acc)[2]) {
+    const double* Xk = X + t.k;
+    const double* sk = s_rate + t.lane * 2;
+    int j = 0;
+    for (; j + 4 <= cmax; j += 4) {
+        uint32_t e[4];
+        double2 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) e[u] = pr_entry(m0, m1, j + u);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            x[u] = make_double2(0.0, 0.0);
+            if (any && j + u < cnt) x[u] = *reinterpret_cast<const double2*>(Xk + (size_t)(ent_slot(e[u]) - base) * Kp);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const double2 r = *reinterpret_cast<const double2*>(sk + ent_rate(e[u]) * 32);
+            acc[0] += r.x * x[u].x;
+            acc[1] += r.y * x[u].y;
+        }
+    }
+    for (; j < cmax; j++) {
+        const uint32_t e = pr_entry(m0, m1, j);
+        double2 x = make_double2(0.0, 0.0);
+        if (any && j < cnt) x = *reinterpret_cast<const double2*>(Xk + (size_t)(ent_slot(e) - base) * Kp);
+        const double2 r = *reinterpret_cast<const double2*>(sk + ent_rate(e) * 32);
+        acc[0] += r.x * x.x;
+        acc[1] += r.y * x.y;
+    }
+}
+
+// this half warp's row r: its entries 0..15 (m0: lane l16 holds entry l16) and 16..31
+// (m1), its entry count, and the larger count of the warp's two rows
+struct PrRow {
+    uint32_t m0, m1;
+    int cnt, cmax;
+};
+__device__ __forceinline__ PrRow pr_row(const SwArgs& a, uint32_t rowbase, uint32_t r, uint32_t count) {
+    PrRow p;
+    const uint32_t l16 = threadIdx.x & 15;
+    uint2 zw = make_uint2(0u, 0u);
+    if (r < count) zw = __ldg(reinterpret_cast<const uint2*>(a.desc + rowbase + r) + 1);
+    p.cnt = (int)zw.y;
+    p.m0 = l16 < zw.y ? __ldg(a.ig_ent + zw.x + l16) : 0u;
+    p.m1 = l16 + 16 < zw.y ? __ldg(a.ig_ent + zw.x + 16 + l16) : 0u;
+    p.cmax = max(p.cnt, __shfl_xor_sync(0xffffffffu, p.cnt, 16));
+    return p;
+}
+
+// Paired-row k_sw_elim: W_e = (sum rate X) / q_e over the group's even rows.
+__global__ void __launch_bounds__(kSwT) k_sw_elim_pr(SwArgs a, const double* __restrict__ X,
+                                                     double* __restrict__ W) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    double* s_rate = reinterpret_cast<double*>(s_raw);
+    const Tile t = tile_of<2>(32);
+    sw_rates(s_rate, a, t);
+    bool act[2];
+    act[0] = !sw_skip(a, t.k);
+    act[1] = !sw_skip(a, t.k + 1);
+    const bool any = act[0] || act[1];
+    if (!__any_sync(0xffffffffu, any)) return;
+    const uint32_t count = a.ne, rs = gridDim.x * t.RB, obase = a.beg + a.ne;
+    // the warp's two rows are rw and rw + 1; the loop condition is warp-uniform
+    for (uint32_t rw = blockIdx.x * t.RB + (t.rsub & ~1); rw < count; rw += rs) {
+        const uint32_t r = rw + (t.rsub & 1);
+        const PrRow p = pr_row(a, a.beg, r, count);
+        double acc[2] = {0.0, 0.0};
+        pr_gathers(s_rate, t, a.Kp, p.m0, p.m1, p.cnt, p.cmax, X, obase, any, acc);
+        if (r < count) {
+            const size_t idx = (size_t)r * a.Kp + t.k;
+            const double2 iq = __ldcs(reinterpret_cast<const double2*>(a.IQe + idx));
+            if (act[0]) W[idx] = acc[0] * iq.x;
+            if (act[1]) W[idx + 1] = acc[1] * iq.y;
+        }
+    }
+}
+
+// Paired-row k_sw_apply, MODE 2 (Y = y, acc0 += AUX . Y, AUX = r0) and MODE 6 (Y = y,
+// acc0 += Y . (AUX X), AUX = dS, acc1 += Y . Y, acc2 += R0x . Y); q_o from Qo.
+template <int MODE>
+__global__ void __launch_bounds__(kSwT) k_sw_apply_pr(SwArgs a, const double* __restrict__ X,
+                                                      const double* __restrict__ W, const double* __restrict__ AUX,
+                                                      double* __restrict__ Y, double* acc0, double* acc1,
+                                                      const double* __restrict__ R0x, double* acc2) {
+    static_assert(MODE == 2 || MODE == 6, "paired-row apply: MODE 2 or 6");
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    double* s_rate = reinterpret_cast<double*>(s_raw);
+    const Tile t = tile_of<2>(32);
+    sw_rates(s_rate, a, t);
+    double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
+    bool act[2];
+    act[0] = !sw_skip(a, t.k);
+    act[1] = !sw_skip(a, t.k + 1);
+    const bool any = act[0] || act[1];
+    if (__any_sync(0xffffffffu, any)) {
+        const uint32_t count = a.no, rs = gridDim.x * t.RB, rowbase = a.beg + a.ne;
+        for (uint32_t rw = blockIdx.x * t.RB + (t.rsub & ~1); rw < count; rw += rs) {
+            const uint32_t r = rw + (t.rsub & 1);
+            const PrRow p = pr_row(a, rowbase, r, count);
+            double flow[2] = {0.0, 0.0};
+            pr_gathers(s_rate, t, a.Kp, p.m0, p.m1, p.cnt, p.cmax, W, a.beg, any, flow);
+            if (r >= count) continue;
+            const size_t i = (size_t)r * a.Kp + t.k;
+            const double2 qv = __ldcs(reinterpret_cast<const double2*>(a.Qo + i));
+            const double2 x = __ldcs(reinterpret_cast<const double2*>(X + i));
+            const double2 aux = __ldcs(reinterpret_cast<const double2*>(AUX + i));
+            const double y0 = qv.x * x.x - flow[0], y1 = qv.y * x.y - flow[1];
+            if (MODE == 2) {
+                if (act[0]) {
+                    __stcs(Y + i, y0);
+                    d0[0] += aux.x * y0;
+                }
+                if (act[1]) {
+                    __stcs(Y + i + 1, y1);
+                    d0[1] += aux.y * y1;
+                }
+            } else {
+                const double2 r0 = __ldcs(reinterpret_cast<const double2*>(R0x + i));
+                if (act[0]) {
+                    __stcs(Y + i, y0);
+                    d0[0] += y0 * (aux.x * x.x);
+                    d1[0] += y0 * y0;
+                    d2[0] += r0.x * y0;
+                }
+                if (act[1]) {
+                    __stcs(Y + i + 1, y1);
+                    d0[1] += y1 * (aux.y * x.y);
+                    d1[1] += y1 * y1;
+                    d2[1] += r0.y * y1;
+                }
+            }
+        }
+    }
+    if (MODE == 6) {
+        double v[3][2] = {{d0[0], d0[1]}, {d1[0], d1[1]}, {d2[0], d2[1]}};
+        double* const dst[3] = {acc0, acc1, acc2};
+        sw_reduce<3, 2>(v, dst, t, a.K);
+    } else {
+        double v[1][2] = {{d0[0], d0[1]}};
+        double* const dst[1] = {acc0};
+        sw_reduce<1, 2>(v, dst, t, a.K);
     }
 }
 
@@ -2125,6 +2294,16 @@ bool debug_on() {
 // Compaction of running systems in the grid-wide groups (ESL_SWEEP_COMPACT=0 turns it
 // off); groups under kCompactMinRows rows are launch-bound and keep their grid.
 constexpr uint32_t kCompactMinRows = 4096;
+// Operator kernels of the 32-system tiles of FP64 grid groups: the paired-row kernels,
+// or one system per lane with ESL_SWEEP_OP=reg
+bool paired_on() {
+    static const bool on = [] {
+        const char* e = getenv("ESL_SWEEP_OP");
+        return !(e && !strcmp(e, "reg"));
+    }();
+    return on;
+}
+
 bool compact_on() {
     static const bool on = [] {
         const char* e = getenv("ESL_SWEEP_COMPACT");
@@ -2521,6 +2700,9 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
             // (not in deflated groups)
             const bool s2 = !defl && a.KT >= 64 && (net->tune_s2 >= 0 ? net->tune_s2 != 0 : ctx->tune_s2 != 0);
             dim3 gei2 = row_grid(g.ne, Kp, a.KT, ctx->sm_count, 2), goi2 = row_grid(g.no, Kp, a.KT, ctx->sm_count, 2);
+            // paired-row kernels on the 32-system tiles of FP64 inner solves (grids gei2 /
+            // goi2: 16 rows per CTA step)
+            const bool paired = inner64 && !defl && paired_on() && a.KT == 32 && a.Qo && a.IQe;
             auto run_inner = [&](auto tag) -> int {
                 using TT = decltype(tag);
                 TT* R = (TT*)vR;
@@ -2580,6 +2762,39 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                                                      d_cnt + 1 + par);
                         }
                         continue;
+                    }
+                    if constexpr (sizeof(TT) == 8) {
+                        if (paired) {
+                            {
+                                ProfScope ps(pc, "schur_operator", op2_bytes);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_elim_pr<<<gei2, kSwT, smT, s>>>(a, PH, WW);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_apply_pr<2><<<goi2, kSwT, smT, s>>>(a, PH, WW, R0, V, sc.c[C_R0V], nullptr, nullptr,
+                                                                        nullptr);
+                            }
+                            {
+                                ProfScope ps(pc, "bicgstab_update", s_bytes);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                            }
+                            {
+                                ProfScope ps(pc, "schur_operator", op6_bytes);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_elim_pr<<<gei2, kSwT, smT, s>>>(a, SH, WW);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_apply_pr<6><<<goi2, kSwT, smT, s>>>(a, SH, WW, dS, Tt, sc.c[C_TS], sc.c[C_TT], R0,
+                                                                        sc.c[C_R0T]);
+                            }
+                            {
+                                ProfScope ps(pc, "bicgstab_update", xrp_bytes);
+                                ESL_COUNT_LAUNCH();
+                                k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                            }
+                            ESL_COUNT_LAUNCH();
+                            k_sw_scal<<<1, 1024, 0, s>>>(a.K, sc, max_iters, kSwStall64, d_cnt + 1 + par);
+                            continue;
+                        }
                     }
                     {
                         ProfScope ps(pc, "schur_operator", op2_bytes);
