@@ -593,73 +593,76 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply(SwArgs a, const T* __restrict
 // deflation, out-rate sums from SwArgs::Qo / IQe.  Tile layout: KT = 32, S = 2, TR = 16
 // (tile_of<2>(32): rsub = threadIdx.x / 16, lane = threadIdx.x % 16).
 
-// entry j (< 32) of this half warp's row, from the row's first 16 entries (m0, lane l16
-// holds entry l16) or the next 16 (m1); j is warp-uniform
-__device__ __forceinline__ uint32_t pr_entry(uint32_t m0, uint32_t m1, int j) {
-    return j < 16 ? __shfl_sync(0xffffffffu, m0, j, 16) : __shfl_sync(0xffffffffu, m1, j - 16, 16);
-}
+// Entries past a row's count are padded with a dummy entry, (base << 6) | 2n: gathered
+// row 0 (always in range) times rate row 2n, a row of zeros the kernels append to the
+// rate table.  So the gather loop needs no predicates; a padded term adds 0 * x.
 
-// acc[q] += sum over this half warp's row's cnt entries of rate(entry) * X[entry row]
-// for this lane's two systems; cmax = the larger count of the warp's two rows.  The sums
-// of inactive systems take whatever their rows hold and are never stored.
+// acc[q] += sum over the entries of this half warp's row (m0: lane l16 holds entry l16,
+// m1: entry 16 + l16, both padded) of rate(entry) * X[entry row] for this lane's two
+// systems; cmax = the larger count of the warp's two rows (warp-uniform).  O32: the
+// gathered vector's element offsets fit in 32 bits.  The sums of inactive systems take
+// whatever their rows hold and are never stored.
+template <bool O32>
 __device__ __forceinline__ void pr_gathers(const double* s_rate, const Tile& t, int Kp, uint32_t m0, uint32_t m1,
-                                           int cnt, int cmax, const double* __restrict__ X, uint32_t base,
-                                           bool any, double (&acc)[2]) {
+                                           int cmax, const double* __restrict__ X, uint32_t base,
+                                           double (&acc)[2]) {
     const double* Xk = X + t.k;
     const double* sk = s_rate + t.lane * 2;
-    int j = 0;
-    for (; j + 4 <= cmax; j += 4) {
-        uint32_t e[4];
-        double2 x[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) e[u] = pr_entry(m0, m1, j + u);
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            x[u] = make_double2(0.0, 0.0);
-            if (any && j + u < cnt) x[u] = *reinterpret_cast<const double2*>(Xk + (size_t)(ent_slot(e[u]) - base) * Kp);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const double2 r = *reinterpret_cast<const double2*>(sk + ent_rate(e[u]) * 32);
-            acc[0] += r.x * x[u].x;
-            acc[1] += r.y * x[u].y;
-        }
-    }
-    for (; j < cmax; j++) {
-        const uint32_t e = pr_entry(m0, m1, j);
-        double2 x = make_double2(0.0, 0.0);
-        if (any && j < cnt) x = *reinterpret_cast<const double2*>(Xk + (size_t)(ent_slot(e) - base) * Kp);
+    auto term = [&](uint32_t e) {
+        const uint32_t row = ent_slot(e) - base;
+        const double* xp = O32 ? Xk + row * (uint32_t)Kp : Xk + (size_t)row * Kp;
+        const double2 x = *reinterpret_cast<const double2*>(xp);
         const double2 r = *reinterpret_cast<const double2*>(sk + ent_rate(e) * 32);
         acc[0] += r.x * x.x;
         acc[1] += r.y * x.y;
+    };
+    const int c16 = min(cmax, 16);
+    int j = 0;
+    // two entries per step: measured faster than four (fewer registers, more warps)
+    for (; j + 2 <= c16; j += 2) {
+        uint32_t e[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) e[u] = __shfl_sync(0xffffffffu, m0, j + u, 16);
+#pragma unroll
+        for (int u = 0; u < 2; u++) term(e[u]);
     }
+    for (; j < c16; j++) term(__shfl_sync(0xffffffffu, m0, j, 16));
+    for (j = 16; j < cmax; j++) term(__shfl_sync(0xffffffffu, m1, j - 16, 16));
 }
 
-// this half warp's row r: its entries 0..15 (m0: lane l16 holds entry l16) and 16..31
-// (m1), its entry count, and the larger count of the warp's two rows
+// this half warp's row r: its padded entries 0..15 (m0) and 16..31 (m1), and the larger
+// entry count of the warp's two rows
 struct PrRow {
     uint32_t m0, m1;
     int cnt, cmax;
 };
-__device__ __forceinline__ PrRow pr_row(const SwArgs& a, uint32_t rowbase, uint32_t r, uint32_t count) {
+__device__ __forceinline__ PrRow pr_row(const SwArgs& a, uint32_t rowbase, uint32_t r, uint32_t count,
+                                        uint32_t dummy) {
     PrRow p;
     const uint32_t l16 = threadIdx.x & 15;
     uint2 zw = make_uint2(0u, 0u);
     if (r < count) zw = __ldg(reinterpret_cast<const uint2*>(a.desc + rowbase + r) + 1);
     p.cnt = (int)zw.y;
-    p.m0 = l16 < zw.y ? __ldg(a.ig_ent + zw.x + l16) : 0u;
-    p.m1 = l16 + 16 < zw.y ? __ldg(a.ig_ent + zw.x + 16 + l16) : 0u;
+    p.m0 = l16 < zw.y ? __ldg(a.ig_ent + zw.x + l16) : dummy;
+    p.m1 = l16 + 16 < zw.y ? __ldg(a.ig_ent + zw.x + 16 + l16) : dummy;
     p.cmax = max(p.cnt, __shfl_xor_sync(0xffffffffu, p.cnt, 16));
     return p;
 }
 
+// rate table of a paired-row kernel: sw_rates plus the zero row 2n of padded entries
+__device__ __forceinline__ void pr_rates(double* s_rate, const SwArgs& a, const Tile& t) {
+    if (threadIdx.x < 32) s_rate[2 * a.n * 32 + threadIdx.x] = 0.0;
+    sw_rates(s_rate, a, t);
+}
+
 // Paired-row k_sw_elim: W_e = (sum rate X) / q_e over the group's even rows.
+template <bool O32>
 __global__ void __launch_bounds__(kSwT) k_sw_elim_pr(SwArgs a, const double* __restrict__ X,
                                                      double* __restrict__ W) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     double* s_rate = reinterpret_cast<double*>(s_raw);
     const Tile t = tile_of<2>(32);
-    sw_rates(s_rate, a, t);
+    pr_rates(s_rate, a, t);
     bool act[2];
     act[0] = !sw_skip(a, t.k);
     act[1] = !sw_skip(a, t.k + 1);
@@ -669,9 +672,9 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim_pr(SwArgs a, const double* __r
     // the warp's two rows are rw and rw + 1; the loop condition is warp-uniform
     for (uint32_t rw = blockIdx.x * t.RB + (t.rsub & ~1); rw < count; rw += rs) {
         const uint32_t r = rw + (t.rsub & 1);
-        const PrRow p = pr_row(a, a.beg, r, count);
+        const PrRow p = pr_row(a, a.beg, r, count, (obase << kEntShift) | (uint32_t)(2 * a.n));
         double acc[2] = {0.0, 0.0};
-        pr_gathers(s_rate, t, a.Kp, p.m0, p.m1, p.cnt, p.cmax, X, obase, any, acc);
+        pr_gathers<O32>(s_rate, t, a.Kp, p.m0, p.m1, p.cmax, X, obase, acc);
         if (r < count) {
             const size_t idx = (size_t)r * a.Kp + t.k;
             const double2 iq = __ldcs(reinterpret_cast<const double2*>(a.IQe + idx));
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_elim_pr(SwArgs a, const double* __r
 
 // Paired-row k_sw_apply, MODE 2 (Y = y, acc0 += AUX . Y, AUX = r0) and MODE 6 (Y = y,
 // acc0 += Y . (AUX X), AUX = dS, acc1 += Y . Y, acc2 += R0x . Y); q_o from Qo.
-template <int MODE>
+template <int MODE, bool O32>
 __global__ void __launch_bounds__(kSwT) k_sw_apply_pr(SwArgs a, const double* __restrict__ X,
                                                       const double* __restrict__ W, const double* __restrict__ AUX,
                                                       double* __restrict__ Y, double* acc0, double* acc1,
@@ -692,7 +695,7 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply_pr(SwArgs a, const double* __
     extern __shared__ __align__(16) unsigned char s_raw[];
     double* s_rate = reinterpret_cast<double*>(s_raw);
     const Tile t = tile_of<2>(32);
-    sw_rates(s_rate, a, t);
+    pr_rates(s_rate, a, t);
     double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0}, d2[2] = {0.0, 0.0};
     bool act[2];
     act[0] = !sw_skip(a, t.k);
@@ -702,9 +705,9 @@ __global__ void __launch_bounds__(kSwT) k_sw_apply_pr(SwArgs a, const double* __
         const uint32_t count = a.no, rs = gridDim.x * t.RB, rowbase = a.beg + a.ne;
         for (uint32_t rw = blockIdx.x * t.RB + (t.rsub & ~1); rw < count; rw += rs) {
             const uint32_t r = rw + (t.rsub & 1);
-            const PrRow p = pr_row(a, rowbase, r, count);
+            const PrRow p = pr_row(a, rowbase, r, count, (a.beg << kEntShift) | (uint32_t)(2 * a.n));
             double flow[2] = {0.0, 0.0};
-            pr_gathers(s_rate, t, a.Kp, p.m0, p.m1, p.cnt, p.cmax, W, a.beg, any, flow);
+            pr_gathers<O32>(s_rate, t, a.Kp, p.m0, p.m1, p.cmax, W, a.beg, flow);
             if (r >= count) continue;
             const size_t i = (size_t)r * a.Kp + t.k;
             const double2 qv = __ldcs(reinterpret_cast<const double2*>(a.Qo + i));
@@ -2703,6 +2706,8 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
             // paired-row kernels on the 32-system tiles of FP64 inner solves (grids gei2 /
             // goi2: 16 rows per CTA step)
             const bool paired = inner64 && !defl && paired_on() && a.KT == 32 && a.Qo && a.IQe;
+            // gathered-vector element offsets (row * Kp) fit in 32 bits
+            const bool o32 = (uint64_t)std::max(g.ne, g.no) * (uint64_t)Kp < (1ull << 31);
             auto run_inner = [&](auto tag) -> int {
                 using TT = decltype(tag);
                 TT* R = (TT*)vR;
@@ -2765,13 +2770,20 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                     }
                     if constexpr (sizeof(TT) == 8) {
                         if (paired) {
+                            // the paired-row kernels' rate table has a zero row appended
+                            const size_t smP = smT + 32 * 8;
                             {
                                 ProfScope ps(pc, "schur_operator", op2_bytes);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_elim_pr<<<gei2, kSwT, smT, s>>>(a, PH, WW);
+                                if (o32) k_sw_elim_pr<true><<<gei2, kSwT, smP, s>>>(a, PH, WW);
+                                else k_sw_elim_pr<false><<<gei2, kSwT, smP, s>>>(a, PH, WW);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_apply_pr<2><<<goi2, kSwT, smT, s>>>(a, PH, WW, R0, V, sc.c[C_R0V], nullptr, nullptr,
-                                                                        nullptr);
+                                if (o32)
+                                    k_sw_apply_pr<2, true><<<goi2, kSwT, smP, s>>>(a, PH, WW, R0, V, sc.c[C_R0V], nullptr,
+                                                                                  nullptr, nullptr);
+                                else
+                                    k_sw_apply_pr<2, false><<<goi2, kSwT, smP, s>>>(a, PH, WW, R0, V, sc.c[C_R0V], nullptr,
+                                                                                   nullptr, nullptr);
                             }
                             {
                                 ProfScope ps(pc, "bicgstab_update", s_bytes);
@@ -2781,10 +2793,15 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                             {
                                 ProfScope ps(pc, "schur_operator", op6_bytes);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_elim_pr<<<gei2, kSwT, smT, s>>>(a, SH, WW);
+                                if (o32) k_sw_elim_pr<true><<<gei2, kSwT, smP, s>>>(a, SH, WW);
+                                else k_sw_elim_pr<false><<<gei2, kSwT, smP, s>>>(a, SH, WW);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_apply_pr<6><<<goi2, kSwT, smT, s>>>(a, SH, WW, dS, Tt, sc.c[C_TS], sc.c[C_TT], R0,
-                                                                        sc.c[C_R0T]);
+                                if (o32)
+                                    k_sw_apply_pr<6, true><<<goi2, kSwT, smP, s>>>(a, SH, WW, dS, Tt, sc.c[C_TS], sc.c[C_TT],
+                                                                                  R0, sc.c[C_R0T]);
+                                else
+                                    k_sw_apply_pr<6, false><<<goi2, kSwT, smP, s>>>(a, SH, WW, dS, Tt, sc.c[C_TS],
+                                                                                   sc.c[C_TT], R0, sc.c[C_R0T]);
                             }
                             {
                                 ProfScope ps(pc, "bicgstab_update", xrp_bytes);
