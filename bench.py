@@ -13,7 +13,9 @@ The metric compares the learned-warm-start + mixed-precision form with the plain
 form.  The headline (`--method direct`, default) is the plain FP64 level sweep, the
 faster of the two on this workload; the learned+mixed form is timed the same way in
 the same run (`learned_mixed`), after its network is trained outside the timed region
-on the plain solves' occupations of the 3,584 training rate sets.
+on the plain solves' occupations of the 3,584 training rate sets.  After the headline
+(outside its steps) the many-network workload runs once through esl_solve_many
+(`many_networks`: 48 networks, n 12-18, 64 x 16 systems each; --no-many skips it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--method direct|learned|mixed|fp64]
     python bench.py --impl reference ...   # the CPU FP64 oracle on the host cores
@@ -361,7 +363,7 @@ def run_ours(args, rank, world, device):
                     "d2h_bytes_per_step": d2h, "wall_s": e2e_wall},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm",
-                         "kernel": "schur_operator (k_sw_elim + k_sw_apply) of the largest level group",
+                         "kernel": "schur_operator (k_sw_elim_pr + k_sw_apply_pr, paired rows) of the largest level group",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None,
                          "peak_kind": peak_kind,
@@ -405,6 +407,67 @@ def cpu_baseline(sample: int, rank: int = 0, world: int = 1, threads: int = 0):
             "sample": f"{sample} of the 512 held-out rate sets, oracle symbolic analysis excluded"}, dt, ref
 
 
+def many_networks(device: int, reps: int = 2):
+    """The many-network workload (48 random networks, n = 12..18, 64 rate sets x 16
+    initial distributions each: 49,152 solves) through one esl_solve_many call over four
+    contexts.  Net.build runs outside the timing; rates and x0 are resident on the
+    device.  Wall clock with the device synchronised on both sides, best of `reps`
+    after one untimed call.  Returns (record, results of the last call)."""
+    import torch
+
+    import paraexastolog_b200 as esl
+    w = synth.config_batch()
+    dev = f"cuda:{device}"
+    ctxs = [esl.Context(device, torch.cuda.Stream(device)) for _ in range(4)]
+    jobs = []
+    for i, (net_g, rates, xs) in enumerate(zip(w.networks, w.rates, w.x0)):
+        net = esl.Net.build(ctxs[i % len(ctxs)], esl.Model.parse(net_g.bnet), rates[0])
+        jobs.append((net, torch.tensor(rates, device=dev), torch.tensor(xs, device=dev)))
+    res = esl.solve_many(ctxs, jobs, method=esl.METHOD_DIRECT, tol=1e-10)
+    times = []
+    for _ in range(reps):
+        del res
+        torch.cuda.synchronize(device)
+        t = time.perf_counter()
+        res = esl.solve_many(ctxs, jobs, method=esl.METHOD_DIRECT, tol=1e-10)
+        torch.cuda.synchronize(device)
+        times.append(time.perf_counter() - t)
+    solves = sum(int(r.x_inf.shape[0]) * int(r.x_inf.shape[1]) for r in res)
+    rec = {"workload": "batch48_n12_18: 48 random networks, n 12-18, 64 rate sets x 16 x0 each",
+           "value": solves / min(times), "unit": "solves/s", "solves": solves, "seconds": min(times),
+           "timing": "wall clock around one esl_solve_many call (4 contexts), device synchronised on both "
+                     "sides; Net.build outside",
+           "converged": all(r.report.converged == 1 and r.status == 0 for r in res)}
+    return rec, w, res
+
+
+def cpu_baseline_many(w, res, n_sample: int = 6):
+    """CPU baseline and accuracy of the many-network workload: the FP64 oracle on a seeded
+    sample of (network, rate set, x0) triples, one host thread each."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle as O
+    rng = np.random.default_rng(48)
+    picks = [(int(i), int(rng.integers(0, 64)), int(rng.integers(0, 16)))
+             for i in rng.choice(len(w.networks), n_sample, replace=False)]
+
+    def one(p):
+        i, b, q = p
+        sym = O.Model(text=w.networks[i].bnet).analyse(w.rates[i][b])
+        t = time.perf_counter()
+        ox, _ = sym.solve(w.x0[i][q], w.rates[i][b])
+        return ox, time.perf_counter() - t
+
+    with ThreadPoolExecutor(n_sample) as ex:
+        refs = list(ex.map(one, picks))
+    l1 = max(float(np.abs(res[i].x_inf[b, q].cpu().numpy() - ox).sum()) for (i, b, q), (ox, _) in zip(picks, refs))
+    cpu_s = sum(dt for _, dt in refs)
+    return ({"value": n_sample / cpu_s, "unit": "solves/s", "cores": 1, "kind": "port",
+             "sample": f"{n_sample} (network, rate set, x0) triples, one thread each; per-core rate, oracle "
+                       "symbolic analysis excluded"},
+            {"solves": n_sample, "l1_max": l1, "target_l1": 1e-9})
+
+
 def run_reference(args):
     # one rate set per host thread, up to 128 threads (~60 MB each): a step takes about
     # one oracle solve (~35 s) however many threads run
@@ -444,6 +507,8 @@ def main():
                     help="skip timing the other form of the comparison (learned+mixed vs plain FP64)")
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-many", action="store_true",
+                    help="skip the many-network workload (48 networks, n 12-18, 64 x 16 systems each)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default level-sweep tiling")
     ap.add_argument("--batch", type=int, default=BATCH, help="held-out rate sets per step (profiling of smaller cases)")
     ap.add_argument("--profile-run", action="store_true",
@@ -511,6 +576,14 @@ def main():
                                                            "maxabs": omx, "target_l1": 1e-9}
     if out is not None:
         out.pop("_other_xinf", None)
+    if world == 1 and not args.no_many and out is not None:
+        # the many-network workload, after the headline (outside its timed steps)
+        del xinf
+        many, w, mres = many_networks(local)
+        if not args.no_cpu_baseline:
+            many["cpu_baseline"], many["accuracy_vs_fp64_oracle"] = cpu_baseline_many(w, mres)
+        del mres
+        out["many_networks"] = many
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
