@@ -92,9 +92,9 @@ def peaks():
 
 
 def traffic_per_byte():
-    """DRAM bytes per algorithmic byte of the Schur operator from the committed ncu
-    capture summary (profiles/schur_operator_traffic.json), or None."""
-    path = os.path.join(REPO, "profiles", "schur_operator_traffic.json")
+    """DRAM bytes per algorithmic byte of the largest group's Schur operator from the
+    committed ncu capture summary (64 systems, two 32-system tiles), or None."""
+    path = os.path.join(REPO, "profiles", "schur_operator_largest_group_n20_x64_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:

@@ -656,8 +656,10 @@ __device__ __forceinline__ void pr_rates(double* s_rate, const SwArgs& a, const 
 }
 
 // Paired-row k_sw_elim: W_e = (sum rate X) / q_e over the group's even rows.
+// 8 CTAs per SM (32 registers, a few bytes of spill): measured faster than 6 CTAs
+// without spill
 template <bool O32>
-__global__ void __launch_bounds__(kSwT) k_sw_elim_pr(SwArgs a, const double* __restrict__ X,
+__global__ void __launch_bounds__(kSwT, 8) k_sw_elim_pr(SwArgs a, const double* __restrict__ X,
                                                      double* __restrict__ W) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     double* s_rate = reinterpret_cast<double*>(s_raw);
@@ -2983,11 +2985,15 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                 ESL_CUDA(cudaGetLastError());
                 return ESL_OK;
             };
+            const int iters_before = group_iters;
             if (inner64) {
                 ESL_TRY(run_inner(double{}));
             } else {
                 ESL_TRY(run_inner(float{}));
             }
+            if (debug_on() && g.ne + g.no > 20000)
+                fprintf(stderr, "[esl-sweep]   round %d: %d systems, %d iterations (%s), %.3f ms\n", outer, h_cnt[0],
+                        group_iters - iters_before, inner64 ? "fp64" : "fp32", g_ms());
             ESL_TRY(true_residual());
             // an FP32 step that no longer halves the residual: continue in FP64
             if (!inner64 && outer >= 2) inner64 = true;
@@ -3022,9 +3028,18 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
         }
         st.relres = std::max(st.relres, worst);
         total_iters += group_iters;
-        if (debug_on())
+        if (debug_on()) {
             fprintf(stderr, "[esl-sweep] group beg %u even %u odd %u max_scc %d: iters %d relres %.3e, %.3f ms\n",
                     g.beg, g.ne, g.no, g.max_scc, group_iters, worst, g_ms());
+            if (g.ne + g.no > 20000) {
+                // Krylov iterations per system over all refinement rounds
+                std::vector<int> its(K);
+                ESL_CUDA(cudaMemcpy(its.data(), sc.i[I_TOTAL], (size_t)K * 4, cudaMemcpyDeviceToHost));
+                std::sort(its.begin(), its.end());
+                fprintf(stderr, "[esl-sweep]   iterations per system: min %d p50 %d p90 %d p99 %d max %d\n",
+                        its.front(), its[K / 2], its[(K * 9) / 10], its[(K * 99) / 100], its.back());
+            }
+        }
     }
     // masses into the terminal SCCs
     a.flags = nullptr;
