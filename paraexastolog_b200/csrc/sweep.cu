@@ -1006,6 +1006,93 @@ __global__ void __launch_bounds__(kSwT) k_sw_xrp(SwArgs a, SwScalPtr sc, T* __re
     sw_reduce<2>(v, dst, t, a.K);
 }
 
+// k_sw_s and k_sw_xrp for FP64 with two adjacent systems per thread (tile_of<2>: 16-byte
+// loads and stores, half the instructions per value; any KT >= 32).  Stores are made for
+// running systems only, as in the one-system kernels.
+__device__ __forceinline__ void st2(double* p, double v0, double v1, bool a0, bool a1) {
+    if (a0 && a1) {
+        __stcs(reinterpret_cast<double2*>(p), make_double2(v0, v1));
+    } else {
+        if (a0) p[0] = v0;
+        if (a1) p[1] = v1;
+    }
+}
+
+__global__ void __launch_bounds__(kSwT) k_sw_s2(SwArgs a, SwScalPtr sc, const double* __restrict__ R,
+                                                const double* __restrict__ V, const double* __restrict__ dS,
+                                                double* __restrict__ SH) {
+    const Tile t = tile_of<2>(a.KT);
+    const bool a0 = !sw_skip(a, t.k), a1 = !sw_skip(a, t.k + 1);
+    if (!a0 && !a1) return;
+    double al[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int k = min(t.k + q, a.Kp - 1);
+        const double r0v = sc.c[C_R0V][k];
+        al[q] = r0v != 0.0 ? sc.c[C_RHO][k] / r0v : 0.0;
+    }
+    for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
+        const size_t idx = (size_t)r * a.Kp + t.k;
+        const double2 rv = __ldcs(reinterpret_cast<const double2*>(R + idx));
+        const double2 vv = __ldcs(reinterpret_cast<const double2*>(V + idx));
+        const double2 dv = __ldcs(reinterpret_cast<const double2*>(dS + idx));
+        st2(SH + idx, (rv.x - al[0] * vv.x) / dv.x, (rv.y - al[1] * vv.y) / dv.y, a0, a1);
+    }
+}
+
+__global__ void __launch_bounds__(kSwT) k_sw_xrp2(SwArgs a, SwScalPtr sc, double* __restrict__ PH,
+                                                  const double* __restrict__ SH, const double* __restrict__ dS,
+                                                  const double* __restrict__ TT, const double* __restrict__ R0,
+                                                  const double* __restrict__ V, double* __restrict__ D,
+                                                  double* __restrict__ R) {
+    const Tile t = tile_of<2>(a.KT);
+    const bool a0 = !sw_skip(a, t.k), a1 = !sw_skip(a, t.k + 1);
+    double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0};
+    if (a0 || a1) {
+        double al[2], om[2], be[2];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int k = min(t.k + q, a.Kp - 1);
+            const double r0v = sc.c[C_R0V][k], tt = sc.c[C_TT][k];
+            al[q] = r0v != 0.0 ? sc.c[C_RHO][k] / r0v : 0.0;
+            om[q] = tt > 0.0 ? sc.c[C_TS][k] / tt : 0.0;
+            be[q] = r0v != 0.0 ? -sc.c[C_R0T][k] / r0v : 0.0;
+        }
+        for (uint32_t r = blockIdx.x * t.RB + t.rsub; r < a.no; r += gridDim.x * t.RB) {
+            const size_t idx = (size_t)r * a.Kp + t.k;
+            const double2 sh = __ldcs(reinterpret_cast<const double2*>(SH + idx));
+            const double2 ph = *reinterpret_cast<const double2*>(PH + idx);
+            const double2 d = __ldcs(reinterpret_cast<const double2*>(dS + idx));
+            const double2 dd = __ldcs(reinterpret_cast<const double2*>(D + idx));
+            const double2 tv = __ldcs(reinterpret_cast<const double2*>(TT + idx));
+            const double2 vv = __ldcs(reinterpret_cast<const double2*>(V + idx));
+            const double2 r0 = __ldcs(reinterpret_cast<const double2*>(R0 + idx));
+            st2(D + idx, dd.x + al[0] * ph.x + om[0] * sh.x, dd.y + al[1] * ph.y + om[1] * sh.y, a0, a1);
+            const double rn0 = d.x * sh.x - om[0] * tv.x, rn1 = d.y * sh.y - om[1] * tv.y;
+            st2(R + idx, rn0, rn1, a0, a1);
+            const double p0 = (rn0 + be[0] * (d.x * ph.x - om[0] * vv.x)) / d.x;
+            const double p1 = (rn1 + be[1] * (d.y * ph.y - om[1] * vv.y)) / d.y;
+            if (a0 && a1) {
+                *reinterpret_cast<double2*>(PH + idx) = make_double2(p0, p1);
+            } else {
+                if (a0) PH[idx] = p0;
+                if (a1) PH[idx + 1] = p1;
+            }
+            if (a0) {
+                d0[0] += rn0 * rn0;
+                d1[0] += r0.x * rn0;
+            }
+            if (a1) {
+                d0[1] += rn1 * rn1;
+                d1[1] += r0.y * rn1;
+            }
+        }
+    }
+    double v[2][2] = {{d0[0], d0[1]}, {d1[0], d1[1]}};
+    double* const dst[2] = {sc.c[C_RR], sc.c[C_RN]};
+    sw_reduce<2, 2>(v, dst, t, a.K);
+}
+
 // Scalar step after each iteration; one CTA; writes the number of running systems.
 __global__ void k_sw_scal(int K, SwScalPtr sc, int max_iters, int stall_max, int* active) {
     __shared__ int s_cnt;
@@ -2796,7 +2883,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                             {
                                 ProfScope ps(pc, "bicgstab_update", s_bytes);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                                k_sw_s2<<<goi2, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
                             }
                             {
                                 ProfScope ps(pc, "schur_operator", op6_bytes);
@@ -2814,7 +2901,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                             {
                                 ProfScope ps(pc, "bicgstab_update", xrp_bytes);
                                 ESL_COUNT_LAUNCH();
-                                k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                                k_sw_xrp2<<<goi2, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                             }
                             ESL_COUNT_LAUNCH();
                             k_sw_scal<<<1, 1024, 0, s>>>(a.K, sc, max_iters, kSwStall64, d_cnt + 1 + par);
@@ -2837,7 +2924,10 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                     {
                         ProfScope ps(pc, "bicgstab_update", s_bytes);
                         ESL_COUNT_LAUNCH();
-                        k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                        if constexpr (sizeof(TT) == 8)
+                            k_sw_s2<<<goi2, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
+                        else
+                            k_sw_s<TT><<<goi, kSwT, 0, s>>>(a, sc, R, V, dS, SH);
                     }
                     {
                         ProfScope ps(pc, "schur_operator", op6_bytes);
@@ -2857,7 +2947,10 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
                     {
                         ProfScope ps(pc, "bicgstab_update", xrp_bytes);
                         ESL_COUNT_LAUNCH();
-                        k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                        if constexpr (sizeof(TT) == 8)
+                            k_sw_xrp2<<<goi2, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
+                        else
+                            k_sw_xrp<TT><<<goi, kSwT, 0, s>>>(a, sc, PH, SH, dS, Tt, R0, V, D, R);
                     }
                     ESL_COUNT_LAUNCH();
                     k_sw_scal<<<1, 1024, 0, s>>>(a.K, sc, max_iters, sizeof(TT) == 8 ? kSwStall64 : kSwStall,
