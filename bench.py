@@ -91,6 +91,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def bf16_peak():
+    """Measured dense bf16 tensor throughput (TFLOP/s, burst), or the fallback."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f).get("bf16_tflops", 1590.0))
+    return 1590.0
+
+
 def traffic_per_byte():
     """DRAM bytes per algorithmic byte of the largest group's Schur operator from the
     committed ncu capture summary (64 systems, two 32-system tiles), or None."""
@@ -275,6 +284,17 @@ def run_ours(args, rank, world, device):
             other["mixed_without_warm_start_iterations"] = cres.report.iterations
             _, pms, _, _ = timed(lambda: mlp.predict(d_rates, out=warm_buf), 3)
             other["warm_start_inference_ms"] = pms / 3
+            # the inference's own roofline: layer 2 (128 x 128) on the tensor cores per
+            # (target state, rate set) sample; layers 1 and 3 are per-sample vector work
+            samples = mlp.n_targets * BATCH
+            flops = 2.0 * 128 * 128 * samples
+            tf = flops / (pms / 3 * 1e-3) / 1e12
+            bf16 = bf16_peak()
+            other["warm_start_inference_roofline"] = {
+                "bound": "tensor", "kernel": "k_mlp_predict (mma.sync m16n8k16 BF16 -> FP32, layer 2)",
+                "samples": samples, "flop_per_sample": 2 * 128 * 128, "achieved": tf, "unit": "TFLOP/s",
+                "peak": bf16, "frac": tf / bf16,
+                "peak_kind": "measured dense bf16 (cuBLAS burst)"}
             other["warm_start_training"] = train_info
 
     # rooflines from live CUDA events on the library's stream: every hot kernel class of
