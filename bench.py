@@ -291,7 +291,7 @@ def run_ours(args, rank, world, device):
             tf = flops / (pms / 3 * 1e-3) / 1e12
             bf16 = bf16_peak()
             other["warm_start_inference_roofline"] = {
-                "bound": "tensor", "kernel": "k_mlp_predict (mma.sync m16n8k16 BF16 -> FP32, layer 2)",
+                "bound": "tensor", "kernel": "k_mlp_predict_tc (tcgen05.mma kind::f16, BF16 -> FP32 in TMEM, layer 2)",
                 "samples": samples, "flop_per_sample": 2 * 128 * 128, "achieved": tf, "unit": "TFLOP/s",
                 "peak": bf16, "frac": tf / bf16,
                 "peak_kind": "measured dense bf16 (cuBLAS burst)"}

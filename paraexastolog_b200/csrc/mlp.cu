@@ -14,9 +14,11 @@
 // [37, 77) log of the 2n rates of k (0 past 2n, 0 for a zero rate).
 // Weights: an FP32 master copy trained with Adam; the forward and backward passes use
 // BF16-rounded weights with FP32 activations and accumulation.  Training runs on SIMT
-// tiled GEMMs; inference runs layer 2 on the tensor cores (mma.sync m16n8k16, BF16 in,
-// FP32 accumulate) with layer 1 split into a per-state part, a per-rate-set part and
-// the log-rate-sum column, so that the 77-wide product is never formed per sample.
+// tiled GEMMs; inference runs layer 2 on the tensor cores (tcgen05.mma with TMEM
+// accumulators, BF16 in, FP32 accumulate; mma.sync m16n8k16 with ESL_MLP_TC=0 or a rate-set
+// count that is not a multiple of 8) with layer 1 split into a per-state part, a
+// per-rate-set part and the log-rate-sum column, so that the 77-wide product is never
+// formed per sample.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -415,6 +417,198 @@ __global__ void __launch_bounds__(128) k_mlp_predict(int nt, int B, int n, size_
     }
 }
 
+// ---- inference with tcgen05 (the default path) -----------------------------------------------
+// A persistent CTA of 128 threads keeps W2 (BF16) in shared memory in the UMMA canonical
+// K-major layout without swizzle.  Per tile of 128 samples:
+//  1. thread t builds its sample's h1 (BF16) into row t of the A tile, in the same layout;
+//  2. one thread issues eight tcgen05.mma (M = 128, N = 128, K = 16 each, kind::f16: BF16
+//     operands from shared memory, FP32 accumulation in 128 TMEM columns) and commits them
+//     to an mbarrier;
+//  3. after that barrier phase completes (a bounded wait), warp w reads TMEM lanes
+//     32w .. 32w + 31 (the rows of its threads' samples) with tcgen05.ld, 16 columns at a
+//     time, and forms y = w3 . relu(acc + b2) + b3 in registers.
+// Canonical K-major layout, no swizzle: an 8-row x 16-byte core matrix is 128 contiguous
+// bytes, and element (r, k) of a 128 x 128 BF16 tile sits at byte
+//   (r % 8) * 16 + (r / 8) * 2048 + (k / 8) * 128 + (k % 8) * 2:
+// core matrices adjacent in K are 128 bytes apart (the descriptor's leading byte offset),
+// those adjacent in M or N 2,048 bytes apart (its stride byte offset), and MMA step s
+// (K = 16 s .. 16 s + 15) starts 256 s bytes into the tile.
+constexpr uint32_t kTcTile = 128;
+constexpr int kTcI = 16, kTcK = 8;  // a tile's target states x rate sets (kTcI * kTcK = kTcTile)
+constexpr uint32_t kTcLBO = 128, kTcSBO = 2048;
+constexpr uint32_t kTcTileBytes = kTcTile * kH * 2;
+constexpr uint32_t kTcWaitLimit = 1u << 22;  // mbarrier polls before a tile is given up
+// instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1), A and B BF16 (bits 7-9
+// and 10-12 = 1), both K-major (bits 15 and 16 = 0), N >> 3 in bits 17-22, M >> 4 in 24-28
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTcTile >> 3) << 17) | ((kTcTile >> 4) << 24);
+
+__device__ __forceinline__ uint32_t tc_off(uint32_t r, uint32_t k) {
+    return (r & 7) * 16 + (r >> 3) * kTcSBO + (k >> 3) * kTcLBO + (k & 7) * 2;
+}
+// shared-memory matrix descriptor: start address, leading and stride byte offsets (each
+// >> 4), descriptor version 1 (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(kTcLBO >> 4) << 16) | ((uint64_t)(kTcSBO >> 4) << 32) |
+           (1ull << 46);
+}
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// polls the mbarrier's phase `parity` at most `limit` times; true once it completed
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, size_t N,
+                                                        const uint32_t* __restrict__ targets,
+                                                        const uint32_t* __restrict__ F,
+                                                        const double* __restrict__ rates,
+                                                        const float* __restrict__ A1, const float* __restrict__ C1,
+                                                        const __nv_bfloat16* __restrict__ W2h,
+                                                        const float* __restrict__ Wq, float mu, float sigma,
+                                                        double* __restrict__ warm, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    unsigned char* sB = tc_smem;                 // W2: row = output feature, column = input
+    unsigned char* sA = tc_smem + kTcTileBytes;  // h1 of the tile's 128 samples
+    __shared__ float sb2[kH], sw3[kH], swq[kH];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t* w2 = reinterpret_cast<const uint32_t*>(W2h);
+    for (int i = tid; i < kH * kH / 2; i += blockDim.x) {
+        const uint32_t r = (uint32_t)i / (kH / 2), k = ((uint32_t)i % (kH / 2)) * 2;
+        *reinterpret_cast<uint32_t*>(sB + tc_off(r, k)) = w2[i];
+    }
+    for (int j = tid; j < kH; j += blockDim.x) {
+        sb2[j] = Wq[oB2 + j];
+        sw3[j] = Wq[oW3 + j];
+        swq[j] = Wq[oW1 + j * kIn + kFq];
+    }
+    const uint32_t bar_a = smem_u32(&bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTcTile)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t tmem_w = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
+    const float b3 = Wq[oB3];
+    const uint32_t sA_a = smem_u32(sA), sB_a = smem_u32(sB);
+    // a tile is 16 target states x 8 rate sets (B is a multiple of 8): its 16 rows of A1
+    // and 8 rows of C1 are read by 8 and 16 threads each, and consecutive tiles of a CTA's
+    // sweep (rate-set blocks fastest) reuse the same A1 rows from L2
+    const long kblocks = B / kTcK, tiles = (long)((nt + kTcI - 1) / kTcI) * kblocks;
+    uint32_t parity = 0;
+    bool ok = true;
+    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long ib = tile / kblocks, kb = tile - ib * kblocks;
+        int i = (int)(ib * kTcI) + tid / kTcK;
+        const int k = (int)(kb * kTcK) + tid % kTcK;
+        const bool valid = i < nt;
+        if (!valid) i = nt - 1;
+        const uint32_t v = targets[i];
+        const float lq = log_rate_sum(v, F[v], rates + (size_t)k * 2 * n);
+        const float* a1 = A1 + (size_t)i * kH;
+        const float* c1 = C1 + (size_t)k * kH;
+#pragma unroll 4
+        for (int c = 0; c < kH / 8; c++) {
+            const float4 p0 = *reinterpret_cast<const float4*>(a1 + 8 * c);
+            const float4 p1 = *reinterpret_cast<const float4*>(a1 + 8 * c + 4);
+            const float4 q0 = *reinterpret_cast<const float4*>(c1 + 8 * c);
+            const float4 q1 = *reinterpret_cast<const float4*>(c1 + 8 * c + 4);
+            const float* w = swq + 8 * c;
+            uint4 pk;
+            pk.x = pack_bf16(fmaxf(p0.x + q0.x + lq * w[0], 0.0f), fmaxf(p0.y + q0.y + lq * w[1], 0.0f));
+            pk.y = pack_bf16(fmaxf(p0.z + q0.z + lq * w[2], 0.0f), fmaxf(p0.w + q0.w + lq * w[3], 0.0f));
+            pk.z = pack_bf16(fmaxf(p1.x + q1.x + lq * w[4], 0.0f), fmaxf(p1.y + q1.y + lq * w[5], 0.0f));
+            pk.w = pack_bf16(fmaxf(p1.z + q1.z + lq * w[6], 0.0f), fmaxf(p1.w + q1.w + lq * w[7], 0.0f));
+            *reinterpret_cast<uint4*>(sA + tc_off((uint32_t)tid, 8u * c)) = pk;
+        }
+        // the tile's h1 (and, at the first tile, W2) becomes visible to the tensor cores
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (uint32_t st = 0; st < kH / 16; st++) {
+                const uint64_t da = tc_desc(sA_a + 256u * st), db = tc_desc(sB_a + 256u * st);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(st), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                         : "memory");
+        }
+        const bool done = tc_wait(bar_a, parity, kTcWaitLimit);
+        parity ^= 1u;
+        if (!__syncthreads_and(done)) {
+            ok = false;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float y = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kH / 16; c++) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem_w + 16u * c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int col = 16 * c + e;
+                y += fmaxf(__uint_as_float(r[e]) + sb2[col], 0.0f) * sw3[col];
+            }
+        }
+        if (valid) {
+            // a non-finite prediction gives no warm start for that entry
+            const double lz = (double)mu + (double)sigma * (double)(y + b3);
+            warm[(size_t)k * N + v] = isfinite(lz) ? exp(fmin(fmax(lz, -700.0), 700.0)) : 0.0;
+        }
+        // every warp's TMEM reads and the MMAs' reads of the A tile are complete before the
+        // next tile overwrites them
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (!ok) {
+        // the tile's MMAs did not complete within the bound: report, give them one more
+        // bounded wait, then release TMEM
+        if (tid == 0) atomicExch(err, 1);
+        tc_wait(bar_a, parity ^ 1u, kTcWaitLimit);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTile) : "memory");
+}
+
 }  // namespace
 }  // namespace esl
 
@@ -435,6 +629,7 @@ struct esl_mlp {
     DevBuf<float> X, H1, H2, dZ2, dZ1, y, dy, ts, ws, C1, Xr, loss;
     DevBuf<int32_t> ks, vs;
     DevBuf<double> stats;
+    DevBuf<int> tc_err;  // timeout flag of the tcgen05 inference
     int cap = 0, cap_b = 0;
 };
 
@@ -761,6 +956,29 @@ int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
     ESL_COUNT_LAUNCH();
     k_mlp_rate_features<<<B, 128, 0, s>>>(B, m->n, d_rates, m->Xr.get());
     ESL_TRY(gemm<G_STORE>(s, B, kH, kIn, m->Xr.get(), kXld, 1, Wq + oW1, 1, kIn, m->C1.get(), kH));
+    // layer 2 on the tcgen05 tensor cores; ESL_MLP_TC=0 selects the mma.sync kernel
+    const char* tc_env = getenv("ESL_MLP_TC");
+    if (!(tc_env && tc_env[0] == '0') && B % kTcK == 0) {
+        ESL_CUDA(cudaFuncSetAttribute(k_mlp_predict_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * kTcTileBytes)));
+        if (!m->tc_err.get()) ESL_TRY(m->tc_err.alloc(1));
+        ESL_CUDA(cudaMemsetAsync(m->tc_err.get(), 0, sizeof(int), s));
+        const long tiles = (long)((m->nt + kTcI - 1) / kTcI) * (B / kTcK);
+        // at most 3 CTAs per SM fit the 66 KB of shared memory, so the 128 TMEM columns of
+        // each stay within the SM's 512
+        const unsigned grid = (unsigned)std::min<long>(tiles, (long)m->ctx->sm_count * 3);
+        ESL_COUNT_LAUNCH();
+        k_mlp_predict_tc<<<grid, 128, 2 * kTcTileBytes, s>>>(m->nt, B, m->n, (size_t)m->N, m->targets.get(),
+                                                             m->net->F.get(), d_rates, m->A1.get(), m->C1.get(),
+                                                             m->W2h.get(), Wq, m->mu, m->sigma, d_warm,
+                                                             m->tc_err.get());
+        ESL_CUDA(cudaGetLastError());
+        int h_err = 0;
+        ESL_CUDA(cudaMemcpyAsync(&h_err, m->tc_err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        ESL_CUDA(cudaStreamSynchronize(s));
+        if (h_err) return fail(ESL_ERR_TIMEOUT, "tensor-core inference: an MMA did not complete in time");
+        return ESL_OK;
+    }
     const long tiles = ((long)m->nt * B + 15) / 16;
     const unsigned grid = (unsigned)std::min<long>((tiles + 3) / 4, (long)m->ctx->sm_count * 16);
     ESL_COUNT_LAUNCH();

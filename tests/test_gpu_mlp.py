@@ -7,7 +7,8 @@
 - the loss and gradient of the training kernels match oracle/mlp.loss_grad (float64,
   same BF16 weights): loss within 1e-4 relative, gradient within 1e-3 in relative norm;
 - the tensor-core inference (BF16 activations) matches the FP32 training forward
-  within 0.05 + 0.02 |y| in standardized log occupation;
+  within 0.05 + 0.02 |y| in standardized log occupation, and its two kernels (tcgen05
+  with TMEM accumulators, the default; mma.sync with ESL_MLP_TC=0) agree within 1e-4;
 - a trained network's warm start is measured against no warm start on held-out rate
   sets, and the warm-started solve still matches the oracle (L1 <= 1e-9).
 """
@@ -141,6 +142,28 @@ def test_tensor_core_inference_matches_forward(esl, ctx, case):
     mask = np.ones(case["net"].N, bool)
     mask[tg] = False
     assert np.all(w[:, mask] == 0.0)
+
+
+def test_tcgen05_and_mma_sync_inference_agree(esl, ctx, case, monkeypatch):
+    # same BF16 operands, FP32 accumulation in a different order: log predictions agree
+    # to rounding; two calls in a row give the same tcgen05 result
+    mlp = esl.Mlp(ctx, case["net"], seed=13)
+    p = mlp.get_params()
+    mlp.set_params(p, 0.0, 1.0)
+    rates = case["rates"][:40]  # a multiple of 8 rate sets: the tcgen05 kernel's tiles
+    w_tc = mlp.predict(rates).cpu().numpy()
+    w_tc2 = mlp.predict(rates).cpu().numpy()
+    monkeypatch.setenv("ESL_MLP_TC", "0")
+    w_mma = mlp.predict(rates).cpu().numpy()
+    monkeypatch.delenv("ESL_MLP_TC")
+    tg = mlp.targets().cpu().numpy()
+    assert np.array_equal(w_tc, w_tc2)
+    a, b = np.log(w_tc[:, tg]), np.log(w_mma[:, tg])
+    assert np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+    assert np.abs(a - b).max() <= 1e-4, np.abs(a - b).max()
+    mask = np.ones(case["net"].N, bool)
+    mask[tg] = False
+    assert np.all(w_tc[:, mask] == 0.0)
 
 
 def test_trained_warm_start_effect(esl, ctx, case, capsys):
