@@ -536,6 +536,9 @@ def main():
     ap.add_argument("--profile-table", action="store_true",
                     help="build the CSC transition tables of the n=20 bench network and of the n=22 drop-in "
                          "network once each, nothing else (for ncu captures of the table kernels)")
+    ap.add_argument("--profile-mlp", action="store_true",
+                    help="run the warm-start inference (untrained weights) of the n=20 bench network on 64 rate "
+                         "sets twice, nothing else (for ncu captures of the tensor-core kernel)")
     args = ap.parse_args()
     BATCH = args.batch
     rank = int(os.environ.get("RANK", "0"))
@@ -551,6 +554,21 @@ def main():
         scale = synth.config_scale()
         for text, r in ((net_g.bnet, rates[0]), (scale.networks[0].bnet, scale.rates[0][0])):
             esl.table(ctx, esl.Model.parse(text), r, with_cols=False)
+        torch.cuda.synchronize()
+        return
+
+    if args.profile_mlp:
+        import torch
+
+        import paraexastolog_b200 as esl
+        ctx = esl.Context(local)
+        net_g, rates, _, _, _ = workload(0, 1)
+        net = esl.Net.build(ctx, esl.Model.parse(net_g.bnet), rates[0])
+        mlp = esl.Mlp(ctx, net, seed=3)
+        mlp.set_params(mlp.get_params(), 0.0, 1.0)
+        d_rates = torch.tensor(rates[:64], device=f"cuda:{local}")
+        for _ in range(2):
+            mlp.predict(d_rates)
         torch.cuda.synchronize()
         return
 

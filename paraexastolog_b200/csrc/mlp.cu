@@ -469,7 +469,17 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, uint32_t 
     return false;
 }
 
-__global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, size_t N,
+// Two groups of 4 warps per CTA, each with its own A tile, mbarrier and 128 TMEM columns,
+// take alternate tiles, so that one group's MMAs and epilogue overlap the other's h1
+// construction.  A group synchronises on its own named barrier (ids 1 and 2).
+__device__ __forceinline__ void tc_group_sync(int g) {
+    if (g == 0)
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+    else
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(256) k_mlp_predict_tc(int nt, int B, int n, size_t N,
                                                         const uint32_t* __restrict__ targets,
                                                         const uint32_t* __restrict__ F,
                                                         const double* __restrict__ rates,
@@ -478,12 +488,15 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
                                                         const float* __restrict__ Wq, float mu, float sigma,
                                                         double* __restrict__ warm, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    unsigned char* sB = tc_smem;                 // W2: row = output feature, column = input
-    unsigned char* sA = tc_smem + kTcTileBytes;  // h1 of the tile's 128 samples
-    __shared__ float sb2[kH], sw3[kH], swq[kH];
-    __shared__ __align__(8) uint64_t bar;
+    unsigned char* sB = tc_smem;  // W2: row = output feature, column = input
+    // read as float4: four columns per shared-memory load in the h1 loop and the head
+    __shared__ __align__(16) float sb2[kH], sw3[kH], swq[kH];
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ int sfail[2];
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = warp >> 2, gt = tid & 127, gw = warp & 3;  // group, thread and warp within it
+    unsigned char* sA = tc_smem + (1 + g) * kTcTileBytes;  // this group's h1 tile
     const uint32_t* w2 = reinterpret_cast<const uint32_t*>(W2h);
     for (int i = tid; i < kH * kH / 2; i += blockDim.x) {
         const uint32_t r = (uint32_t)i / (kH / 2), k = ((uint32_t)i % (kH / 2)) * 2;
@@ -494,14 +507,15 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
         sw3[j] = Wq[oW3 + j];
         swq[j] = Wq[oW1 + j * kIn + kFq];
     }
-    const uint32_t bar_a = smem_u32(&bar);
+    const uint32_t bar_a = smem_u32(&bar[g]);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(kTcTile)
+                     "r"(2 * kTcTile)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -509,7 +523,8 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const uint32_t tmem_w = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
+    const uint32_t tmem_g = tmem + (uint32_t)g * kTcTile;           // this group's accumulator
+    const uint32_t tmem_w = tmem_g + ((uint32_t)(gw * 32) << 16);  // this warp's lanes of it
     const float b3 = Wq[oB3];
     const uint32_t sA_a = smem_u32(sA), sB_a = smem_u32(sB);
     // a tile is 16 target states x 8 rate sets (B is a multiple of 8): its 16 rows of A1
@@ -518,12 +533,13 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
     const long kblocks = B / kTcK, tiles = (long)((nt + kTcI - 1) / kTcI) * kblocks;
     uint32_t parity = 0;
     bool ok = true;
-    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (long tile = 2L * blockIdx.x + g; tile < tiles; tile += 2L * gridDim.x) {
         const long ib = tile / kblocks, kb = tile - ib * kblocks;
-        int i = (int)(ib * kTcI) + tid / kTcK;
-        const int k = (int)(kb * kTcK) + tid % kTcK;
+        int i = (int)(ib * kTcI) + gt / kTcK;
+        const int k = (int)(kb * kTcK) + gt % kTcK;
         const bool valid = i < nt;
         if (!valid) i = nt - 1;
+        if (gt == 0) sfail[g] = 0;
         const uint32_t v = targets[i];
         const float lq = log_rate_sum(v, F[v], rates + (size_t)k * 2 * n);
         const float* a1 = A1 + (size_t)i * kH;
@@ -534,18 +550,19 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
             const float4 p1 = *reinterpret_cast<const float4*>(a1 + 8 * c + 4);
             const float4 q0 = *reinterpret_cast<const float4*>(c1 + 8 * c);
             const float4 q1 = *reinterpret_cast<const float4*>(c1 + 8 * c + 4);
-            const float* w = swq + 8 * c;
+            const float4 w0 = *reinterpret_cast<const float4*>(swq + 8 * c);
+            const float4 w1 = *reinterpret_cast<const float4*>(swq + 8 * c + 4);
             uint4 pk;
-            pk.x = pack_bf16(fmaxf(p0.x + q0.x + lq * w[0], 0.0f), fmaxf(p0.y + q0.y + lq * w[1], 0.0f));
-            pk.y = pack_bf16(fmaxf(p0.z + q0.z + lq * w[2], 0.0f), fmaxf(p0.w + q0.w + lq * w[3], 0.0f));
-            pk.z = pack_bf16(fmaxf(p1.x + q1.x + lq * w[4], 0.0f), fmaxf(p1.y + q1.y + lq * w[5], 0.0f));
-            pk.w = pack_bf16(fmaxf(p1.z + q1.z + lq * w[6], 0.0f), fmaxf(p1.w + q1.w + lq * w[7], 0.0f));
-            *reinterpret_cast<uint4*>(sA + tc_off((uint32_t)tid, 8u * c)) = pk;
+            pk.x = pack_bf16(fmaxf(p0.x + q0.x + lq * w0.x, 0.0f), fmaxf(p0.y + q0.y + lq * w0.y, 0.0f));
+            pk.y = pack_bf16(fmaxf(p0.z + q0.z + lq * w0.z, 0.0f), fmaxf(p0.w + q0.w + lq * w0.w, 0.0f));
+            pk.z = pack_bf16(fmaxf(p1.x + q1.x + lq * w1.x, 0.0f), fmaxf(p1.y + q1.y + lq * w1.y, 0.0f));
+            pk.w = pack_bf16(fmaxf(p1.z + q1.z + lq * w1.z, 0.0f), fmaxf(p1.w + q1.w + lq * w1.w, 0.0f));
+            *reinterpret_cast<uint4*>(sA + tc_off((uint32_t)gt, 8u * c)) = pk;
         }
         // the tile's h1 (and, at the first tile, W2) becomes visible to the tensor cores
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+        tc_group_sync(g);
+        if (gt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
             for (uint32_t st = 0; st < kH / 16; st++) {
@@ -555,15 +572,16 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
                     "setp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
                     :
-                    : "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(st), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "r"(tmem_g), "l"(da), "l"(db), "r"(kTcIdesc), "r"(st), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
                          : "memory");
         }
-        const bool done = tc_wait(bar_a, parity, kTcWaitLimit);
+        if (!tc_wait(bar_a, parity, kTcWaitLimit)) sfail[g] = 1;
         parity ^= 1u;
-        if (!__syncthreads_and(done)) {
+        tc_group_sync(g);
+        if (sfail[g]) {  // the same for every thread of the group
             ok = false;
             break;
         }
@@ -581,9 +599,13 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
                 : "r"(tmem_w + 16u * c));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
-                const int col = 16 * c + e;
-                y += fmaxf(__uint_as_float(r[e]) + sb2[col], 0.0f) * sw3[col];
+            for (int e = 0; e < 16; e += 4) {
+                const float4 bb = *reinterpret_cast<const float4*>(sb2 + 16 * c + e);
+                const float4 ww = *reinterpret_cast<const float4*>(sw3 + 16 * c + e);
+                y += fmaxf(__uint_as_float(r[e]) + bb.x, 0.0f) * ww.x;
+                y += fmaxf(__uint_as_float(r[e + 1]) + bb.y, 0.0f) * ww.y;
+                y += fmaxf(__uint_as_float(r[e + 2]) + bb.z, 0.0f) * ww.z;
+                y += fmaxf(__uint_as_float(r[e + 3]) + bb.w, 0.0f) * ww.w;
             }
         }
         if (valid) {
@@ -591,22 +613,23 @@ __global__ void __launch_bounds__(128) k_mlp_predict_tc(int nt, int B, int n, si
             const double lz = (double)mu + (double)sigma * (double)(y + b3);
             warm[(size_t)k * N + v] = isfinite(lz) ? exp(fmin(fmax(lz, -700.0), 700.0)) : 0.0;
         }
-        // every warp's TMEM reads and the MMAs' reads of the A tile are complete before the
+        // the group's TMEM reads and its MMAs' reads of the A tile are complete before the
         // next tile overwrites them
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
+        tc_group_sync(g);
     }
     if (!ok) {
         // the tile's MMAs did not complete within the bound: report, give them one more
         // bounded wait, then release TMEM
-        if (tid == 0) atomicExch(err, 1);
+        if (gt == 0) atomicExch(err, 1);
         tc_wait(bar_a, parity ^ 1u, kTcWaitLimit);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTile) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcTile)
+                     : "memory");
 }
 
 }  // namespace
@@ -960,15 +983,15 @@ int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
     const char* tc_env = getenv("ESL_MLP_TC");
     if (!(tc_env && tc_env[0] == '0') && B % kTcK == 0) {
         ESL_CUDA(cudaFuncSetAttribute(k_mlp_predict_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * kTcTileBytes)));
+                                      (int)(3 * kTcTileBytes)));
         if (!m->tc_err.get()) ESL_TRY(m->tc_err.alloc(1));
         ESL_CUDA(cudaMemsetAsync(m->tc_err.get(), 0, sizeof(int), s));
         const long tiles = (long)((m->nt + kTcI - 1) / kTcI) * (B / kTcK);
-        // at most 3 CTAs per SM fit the 66 KB of shared memory, so the 128 TMEM columns of
+        // at most 2 CTAs per SM fit the 98 KB of shared memory, so the 256 TMEM columns of
         // each stay within the SM's 512
-        const unsigned grid = (unsigned)std::min<long>(tiles, (long)m->ctx->sm_count * 3);
+        const unsigned grid = (unsigned)std::min<long>((tiles + 1) / 2, (long)m->ctx->sm_count * 2);
         ESL_COUNT_LAUNCH();
-        k_mlp_predict_tc<<<grid, 128, 2 * kTcTileBytes, s>>>(m->nt, B, m->n, (size_t)m->N, m->targets.get(),
+        k_mlp_predict_tc<<<grid, 256, 3 * kTcTileBytes, s>>>(m->nt, B, m->n, (size_t)m->N, m->targets.get(),
                                                              m->net->F.get(), d_rates, m->A1.get(), m->C1.get(),
                                                              m->W2h.get(), Wq, m->mu, m->sigma, d_warm,
                                                              m->tc_err.get());
