@@ -100,6 +100,9 @@ struct SweepPlan {
     DevBuf<uint32_t> og_ptr, og_ent;     // predecessors in earlier groups
     DevBuf<uint32_t> tp_ptr, tp_ent;     // transient predecessors of terminal position p
     DevBuf<uint32_t> lsc_off;            // local SCCs: offsets into lsc_slots
+    // local SCCs: per CTA-local group, its SCCs' group-relative indices by decreasing
+    // size (the launch order of k_sw_local), or empty
+    DevBuf<uint32_t> lsc_rank;
     DevBuf<uint32_t> lsc_ne;             // local SCCs: number of even-parity slots (listed first)
     DevBuf<uint32_t> lsc_slots;          // local SCCs: slots, SCC by SCC
     // terminal plan: per slot, the state's position in the reordering
@@ -1269,6 +1272,9 @@ struct SwLocal {
     unsigned long long* ratio;  // per system: max over SCCs of final |r|^2 / |b|^2 (bits of a double >= 0)
     int* fail;                  // per system: 1 once an SCC stays above the acceptance residual
     int* iters;                 // per system: inner iterations, max over SCCs
+    // the SCC at place p of the launch order is the group's SCC rank[p] (largest first),
+    // or SCC p when null
+    const uint32_t* rank;
 };
 
 struct LocalRows {
@@ -1444,17 +1450,22 @@ __global__ void __launch_bounds__(kSwLocalWarps * 32) k_sw_local(SwArgs a, SwLoc
     t.lane = threadIdx.x & 31;
     t.rsub = threadIdx.x >> 5;
     t.RB = blockDim.x >> 5;
-    t.k = blockIdx.y * 32 + t.lane;
+    // CTA b solves 32-system tile b % tiles of the SCC at place b / tiles in the launch
+    // order: every tile of the largest SCCs is dispatched first, so that the CTAs with
+    // the longest refinements do not start in a late wave
+    const uint32_t tiles = (uint32_t)a.Kp / 32, tile = blockIdx.x % tiles, place = blockIdx.x / tiles;
+    const uint32_t j = l.rank ? l.rank[place] : place;
+    t.k = tile * 32 + t.lane;
     for (int idx = threadIdx.x; idx < 2 * a.n * 32; idx += blockDim.x) {
-        const double r = a.rateT[(size_t)(idx >> 5) * a.Kp + blockIdx.y * 32 + (idx & 31)];
+        const double r = a.rateT[(size_t)(idx >> 5) * a.Kp + tile * 32 + (idx & 31)];
         s64[idx] = r;
         s32[idx] = (float)r;
     }
     __syncthreads();
-    const uint32_t off = l.off[blockIdx.x];
+    const uint32_t off = l.off[j];
     LocalRows L;
-    L.se = (int)l.ne[blockIdx.x];
-    L.so = (int)(l.off[blockIdx.x + 1] - off) - L.se;
+    L.se = (int)l.ne[j];
+    L.so = (int)(l.off[j + 1] - off) - L.se;
     L.ev = l.slots + off;
     L.od = L.ev + L.se;
     L.warp = t.rsub;
@@ -2295,6 +2306,34 @@ int build_plan_device(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     return ESL_OK;
 }
 
+// Launch order of the CTA-local groups: per group, its SCCs' group-relative indices by
+// decreasing size (ties by index), read by k_sw_local through SwLocal::rank.  A group
+// lasts as long as its slowest CTA, the one of its largest SCC; started first, that CTA
+// no longer waits for a free slot behind the small ones.
+int build_local_rank(esl_ctx* ctx, SweepPlan* P) {
+    uint32_t nl = 0;
+    for (const SwGroup& g : P->groups)
+        if (g.kind == 1) nl = std::max(nl, g.scc0 + g.nscc);
+    if (nl == 0) return ESL_OK;
+    cudaStream_t s = ctx->stream;
+    std::vector<uint32_t> off((size_t)nl + 1), rank(nl);
+    ESL_CUDA(cudaMemcpyAsync(off.data(), P->lsc_off.get(), ((size_t)nl + 1) * 4, cudaMemcpyDeviceToHost, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    for (const SwGroup& g : P->groups) {
+        if (g.kind != 1) continue;
+        std::vector<uint32_t> idx(g.nscc);
+        for (uint32_t j = 0; j < g.nscc; j++) idx[j] = j;
+        std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+            return off[g.scc0 + x + 1] - off[g.scc0 + x] > off[g.scc0 + y + 1] - off[g.scc0 + y];
+        });
+        std::copy(idx.begin(), idx.end(), rank.begin() + g.scc0);
+    }
+    ESL_TRY(P->lsc_rank.alloc(nl));
+    ESL_CUDA(cudaMemcpyAsync(P->lsc_rank.get(), rank.data(), (size_t)nl * 4, cudaMemcpyHostToDevice, s));
+    ESL_CUDA(cudaStreamSynchronize(s));
+    return ESL_OK;
+}
+
 int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     // one builder at a time, so that threads solving the same network share one plan
     static std::mutex mu;
@@ -2305,6 +2344,10 @@ int build_plan(esl_ctx* ctx, const esl_net* net, SweepPlan*& out) {
     }
     SweepPlan* P = nullptr;
     ESL_TRY(build_plan_device(ctx, net, P));
+    if (int rc = build_local_rank(ctx, P); rc != ESL_OK) {
+        delete P;
+        return rc;
+    }
     esl_net* mnet = const_cast<esl_net*>(net);
     mnet->sweep = P;
     mnet->sweep_free = free_plan_sweep;
@@ -2663,6 +2706,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
         if (g.kind == 1) {
             SwLocal l{};
             l.off = P->lsc_off.get() + g.scc0;
+            l.rank = P->lsc_rank.get() ? P->lsc_rank.get() + g.scc0 : nullptr;
             l.ne = P->lsc_ne.get() + g.scc0;
             l.slots = P->lsc_slots.get();
             l.bS = bS;
@@ -2698,7 +2742,7 @@ int sweep_run(esl_ctx* ctx, const esl_net* net, SweepPlan* P, bool term, int K, 
             const size_t smem = (size_t)2 * n * 32 * (8 + 4);
             if (g.nscc > 0) {
                 ESL_COUNT_LAUNCH();
-                k_sw_local<<<dim3(g.nscc, Kp / 32), nw * 32, smem, s>>>(a, l);
+                k_sw_local<<<(unsigned)g.nscc * (unsigned)(Kp / 32), nw * 32, smem, s>>>(a, l);
             }
             // even rows of the group from the odd solution, straight into Z
             a.flags = nullptr;
