@@ -438,6 +438,7 @@ constexpr int kTcI = 16, kTcK = 8;  // a tile's target states x rate sets (kTcI 
 constexpr uint32_t kTcLBO = 128, kTcSBO = 2048;
 constexpr uint32_t kTcTileBytes = kTcTile * kH * 2;
 constexpr uint32_t kTcWaitLimit = 1u << 22;  // mbarrier polls before a tile is given up
+constexpr uint32_t kTcTestWaitLimit = 1u << 10;  // the same when the timeout path is tested
 // instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1), A and B BF16 (bits 7-9
 // and 10-12 = 1), both K-major (bits 15 and 16 = 0), N >> 3 in bits 17-22, M >> 4 in 24-28
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTcTile >> 3) << 17) | ((kTcTile >> 4) << 24);
@@ -486,7 +487,8 @@ __global__ void __launch_bounds__(256) k_mlp_predict_tc(int nt, int B, int n, si
                                                         const float* __restrict__ A1, const float* __restrict__ C1,
                                                         const __nv_bfloat16* __restrict__ W2h,
                                                         const float* __restrict__ Wq, float mu, float sigma,
-                                                        double* __restrict__ warm, int* __restrict__ err) {
+                                                        double* __restrict__ warm, int* __restrict__ err,
+                                                        int no_mma) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     unsigned char* sB = tc_smem;  // W2: row = output feature, column = input
     // read as float4: four columns per shared-memory load in the h1 loop and the head
@@ -562,7 +564,9 @@ __global__ void __launch_bounds__(256) k_mlp_predict_tc(int nt, int B, int n, si
         // the tile's h1 (and, at the first tile, W2) becomes visible to the tensor cores
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_group_sync(g);
-        if (gt == 0) {
+        // no_mma (a test of the timeout path): nothing is issued, so the wait below runs
+        // out with no tensor-core work in flight
+        if (gt == 0 && !no_mma) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
             for (uint32_t st = 0; st < kH / 16; st++) {
@@ -578,7 +582,7 @@ __global__ void __launch_bounds__(256) k_mlp_predict_tc(int nt, int B, int n, si
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
                          : "memory");
         }
-        if (!tc_wait(bar_a, parity, kTcWaitLimit)) sfail[g] = 1;
+        if (!tc_wait(bar_a, parity, no_mma ? kTcTestWaitLimit : kTcWaitLimit)) sfail[g] = 1;
         parity ^= 1u;
         tc_group_sync(g);
         if (sfail[g]) {  // the same for every thread of the group
@@ -622,7 +626,7 @@ __global__ void __launch_bounds__(256) k_mlp_predict_tc(int nt, int B, int n, si
         // the tile's MMAs did not complete within the bound: report, give them one more
         // bounded wait, then release TMEM
         if (gt == 0) atomicExch(err, 1);
-        tc_wait(bar_a, parity ^ 1u, kTcWaitLimit);
+        tc_wait(bar_a, parity ^ 1u, no_mma ? kTcTestWaitLimit : kTcWaitLimit);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -982,6 +986,10 @@ int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
     // layer 2 on the tcgen05 tensor cores; ESL_MLP_TC=0 selects the mma.sync kernel
     const char* tc_env = getenv("ESL_MLP_TC");
     if (!(tc_env && tc_env[0] == '0') && B % kTcK == 0) {
+        // ESL_MLP_TC_TIMEOUT_TEST=1 issues no MMAs, so that the kernel's bounded wait runs
+        // out and the call returns ESL_ERR_TIMEOUT (a test of that path; read per call)
+        const char* tt_env = getenv("ESL_MLP_TC_TIMEOUT_TEST");
+        const int no_mma = (tt_env && tt_env[0] == '1') ? 1 : 0;
         ESL_CUDA(cudaFuncSetAttribute(k_mlp_predict_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(3 * kTcTileBytes)));
         if (!m->tc_err.get()) ESL_TRY(m->tc_err.alloc(1));
@@ -994,7 +1002,7 @@ int esl_mlp_predict(esl_mlp* m, int B, const double* d_rates, double* d_warm) {
         k_mlp_predict_tc<<<grid, 256, 3 * kTcTileBytes, s>>>(m->nt, B, m->n, (size_t)m->N, m->targets.get(),
                                                              m->net->F.get(), d_rates, m->A1.get(), m->C1.get(),
                                                              m->W2h.get(), Wq, m->mu, m->sigma, d_warm,
-                                                             m->tc_err.get());
+                                                             m->tc_err.get(), no_mma);
         ESL_CUDA(cudaGetLastError());
         int h_err = 0;
         ESL_CUDA(cudaMemcpyAsync(&h_err, m->tc_err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));

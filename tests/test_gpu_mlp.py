@@ -9,6 +9,8 @@
 - the tensor-core inference (BF16 activations) matches the FP32 training forward
   within 0.05 + 0.02 |y| in standardized log occupation, and its two kernels (tcgen05
   with TMEM accumulators, the default; mma.sync with ESL_MLP_TC=0) agree within 1e-4;
+- the tcgen05 kernel's bounded mbarrier wait, made to run out, returns ESL_ERR_TIMEOUT
+  and leaves the context usable;
 - a trained network's warm start is measured against no warm start on held-out rate
   sets, and the warm-started solve still matches the oracle (L1 <= 1e-9).
 """
@@ -164,6 +166,22 @@ def test_tcgen05_and_mma_sync_inference_agree(esl, ctx, case, monkeypatch):
     mask = np.ones(case["net"].N, bool)
     mask[tg] = False
     assert np.all(w_tc[:, mask] == 0.0)
+
+
+def test_tcgen05_wait_timeout_is_reported(esl, ctx, case, monkeypatch):
+    # The tcgen05 kernel's mbarrier wait is bounded.  ESL_MLP_TC_TIMEOUT_TEST=1 issues no
+    # MMA, so the wait runs out with no tensor-core work in flight: the call returns
+    # ESL_ERR_TIMEOUT, and the context stays usable (the next call predicts as before).
+    mlp = esl.Mlp(ctx, case["net"], seed=13)
+    mlp.set_params(mlp.get_params(), 0.0, 1.0)
+    rates = case["rates"][:40]
+    ref = mlp.predict(rates).cpu().numpy()
+    monkeypatch.setenv("ESL_MLP_TC_TIMEOUT_TEST", "1")
+    with pytest.raises(esl.EslError) as e:
+        mlp.predict(rates)
+    assert e.value.code == -5  # ESL_ERR_TIMEOUT
+    monkeypatch.delenv("ESL_MLP_TC_TIMEOUT_TEST")
+    assert np.array_equal(mlp.predict(rates).cpu().numpy(), ref)
 
 
 def test_trained_warm_start_effect(esl, ctx, case, capsys):
