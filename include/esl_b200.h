@@ -243,6 +243,8 @@ int esl_solve_host(esl_ctx* ctx, const esl_model* m, int B, const double* rates,
  *      b2[128], w3[128], b3 (FP32 master copy). */
 #define ESL_MLP_PARAMS 26625
 int esl_mlp_create(esl_ctx* ctx, const esl_net* net, uint64_t seed, esl_mlp** out);
+/* waits for the device, then frees; touches neither the context nor the net, so it may
+ * come after either has been freed */
 int esl_mlp_free(esl_mlp* mlp);
 /* number of states it predicts (odd-parity rows of the grid-wide level groups) and the
  * label standardisation log z = mu + sigma * y */

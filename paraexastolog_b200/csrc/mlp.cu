@@ -826,11 +826,13 @@ int esl_mlp_create(esl_ctx* ctx, const esl_net* net, uint64_t seed, esl_mlp** ou
 }
 
 int esl_mlp_free(esl_mlp* m) {
-    StreamScope stream_scope_(m ? m->ctx : nullptr);
-    if (m) {
-        cudaStreamSynchronize(m->ctx->stream);
-        delete m;
-    }
+    if (!m) return ESL_OK;
+    // as esl_net_free: one device-wide wait, and the context is not touched, so that an
+    // mlp may be freed after its context (a garbage collector frees them in any order)
+    cudaDeviceSynchronize();
+    t_released_synced = true;
+    delete m;
+    t_released_synced = false;
     return ESL_OK;
 }
 
